@@ -1,0 +1,402 @@
+"""Benchmark of the spmv_b200 hot path (one JSON line on rank 0).
+
+Workload (default): 3D 7-point Laplacian on 128^3 (2,097,152 rows,
+14,581,760 nnz), FP64 CSR with int32 indices, split into 8 row-block ranks with
+L2GMap ghosts on one GPU; b ~ U[-1,1] (seed 1); x0 = 0.
+
+A step is one FP64 CG solve to relative residual 1e-8 through spmv::cg's
+device path (b and x device-resident).  `value` = solves/s over the whole job.
+`e2e` is the same solve through the C ABI with pinned host b and x (the
+host->device copy of b and device->host copy of x inside the timed region).
+`roofline` covers the dominant kernel, the CSR product, timed live with CUDA
+events on the library's stream over repeated launches of Matrix::mult.
+
+`--impl reference` times the reference's CPU path instead: the oracle's
+restatement of spmv::cg (Eigen/MKL/MPI are not available to build the real
+reference) on all host threads, one bounded sample of CG iterations per step.
+
+Multi-GPU (torchrun, N > 1): replicas only.  Each rank solves its own copy of
+the workload on its own GPU (no data-path collective); `value` sums solves over
+ranks divided by the max-over-ranks time ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "c2"
+MEASURED_PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+L2_BYTES = 126 * 2 ** 20
+
+
+def peaks():
+    try:
+        d = json.loads(MEASURED_PEAKS.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self._t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) != 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[2:]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# Workload
+# ---------------------------------------------------------------------------
+def spmv_bytes(n, nnz, P, g, sv=8, si=4):
+    """Algorithmic bytes of one update + SpMV (values+cols, rowptr per rank,
+    x owned+ghost read once, y written once, ghost gather)."""
+    return nnz * (sv + si) + (n + P) * si + (n + g) * sv + n * sv + g * (2 * sv + si)
+
+
+def kernel_bytes(n, nnz, P, g, sv=8, si=4):
+    """Algorithmic bytes of the product kernel alone (no ghost gather)."""
+    return nnz * (sv + si) + (n + P) * si + (n + g) * sv + n * sv
+
+
+def setup(device: int):
+    import spmv_b200 as S
+    from spmv_b200 import gen
+    W = gen.workload(WORKLOAD)
+    D = gen.distribute(W.A, W.P)
+    comm = S.Comm(size=W.P, device=device)
+    cm = S.L2GMap(comm, D.local_sizes, D.ghosts)
+    rm = S.L2GMap(comm, D.local_sizes, [[] for _ in range(W.P)])
+    M = S.Matrix(comm, D.blocks, cm, rm)
+    return W, D, comm, cm, rm, M
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=None)
+    return world, rank, local
+
+
+def max_over_ranks(v: float, world: int, device: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{device}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int, device: int):
+    import torch
+    torch.cuda.synchronize(device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier(device_ids=[device])
+        torch.cuda.synchronize(device)
+
+
+def cpu_sample(W, D, budget_s: float, nthreads: int):
+    """Times the oracle's spmv::cg (all host threads) for a bounded number of
+    iterations; returns (seconds per iteration, iterations run)."""
+    import oracle
+    om = oracle.Map(D.local_sizes, D.ghosts)
+    b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(D.P)]
+    t0 = time.perf_counter()
+    oracle.cg(om, D.blocks, b, 10000, W.rtol, nthreads=nthreads, max_its_run=3)
+    per = (time.perf_counter() - t0) / 3
+    its = int(max(3, min(2000, budget_s / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    _, k, _ = oracle.cg(om, D.blocks, b, 10000, W.rtol, nthreads=nthreads,
+                        max_its_run=its)
+    dt = time.perf_counter() - t0
+    return dt / k, k
+
+
+def config_dict(W, D, P, extra=None):
+    g = int(sum(len(x) for x in D.ghosts))
+    c = {"workload": "3D 7-point Laplacian 128^3 (c2): n=2097152, nnz=14581760, "
+                     "8 row-block ranks on one GPU, ghosts=%d; FP64 CG to rel-res 1e-8, "
+                     "b~U[-1,1] seed 1" % g,
+         "n": W.A.nrows, "nnz": W.A.nnz, "ranks": P, "ghosts": g, "rtol": W.rtol,
+         "l2": "working set (matrix 223 MB + CG vectors) exceeds the 126 MB L2; "
+               "no flush between steps",
+         "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# Reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from spmv_b200 import gen
+    import oracle
+    W = gen.workload(WORKLOAD)
+    D = gen.distribute(W.A, W.P)
+    nthreads = oracle.max_threads()
+    k_full = 441  # iterations of the oracle's FP64 CG on this workload
+    per_step = []
+    for i in range(args.warmup + args.steps):
+        spi, its = cpu_sample(W, D, args.ref_budget, nthreads)
+        if i >= args.warmup:
+            per_step.append(spi * k_full)
+    t = float(np.mean(per_step))
+    value = 1.0 / t
+    sample = ("oracle spmv::cg restatement, %d threads; each step times a bounded "
+              "run of CG iterations (~%.0f s) and scales to the %d iterations of a "
+              "full solve" % (nthreads, args.ref_budget, k_full))
+    line = {"impl": "reference", "metric": "CG solves/s", "value": value,
+            "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": config_dict(W, D, W.P),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import torch
+    import spmv_b200 as S
+    device = local
+    torch.cuda.set_device(device)
+    W, D, comm, cm, rm, M = setup(device)
+    P = W.P
+    stream = torch.cuda.ExternalStream(comm.stream, device=f"cuda:{device}")
+    n, nnz = W.A.nrows, W.A.nnz
+    g = int(sum(len(x) for x in D.ghosts))
+
+    # Device-resident inputs.
+    bd = [torch.from_numpy(W.b[D.ranges[q]:D.ranges[q + 1]].copy()).cuda(device)
+          for q in range(P)]
+    xd = [torch.zeros(cm.vec_len(q), dtype=torch.float64, device=f"cuda:{device}")
+          for q in range(P)]
+
+    # --- value: K device-resident solves ---------------------------------
+    k_its = None
+    for _ in range(args.warmup):
+        _, k_its = S.cg(comm, M, bd, 10000, W.rtol, x=xd)
+    clocks = ClockSampler(device)
+    barrier(world, device)
+    clocks.start()
+    t_ev0 = torch.cuda.Event(enable_timing=True)
+    t_ev1 = torch.cuda.Event(enable_timing=True)
+    t_ev0.record(stream)
+    its = []
+    for _ in range(args.steps):
+        _, k = S.cg(comm, M, bd, 10000, W.rtol, x=xd)
+        its.append(k)
+    t_ev1.record(stream)
+    torch.cuda.synchronize(device)
+    clk = clocks.stop()
+    barrier(world, device)
+    t_local = t_ev0.elapsed_time(t_ev1) / 1e3
+    t_max = max_over_ranks(t_local, world, device)
+    value = world * args.steps / t_max
+    k_mean = float(np.mean(its))
+
+    # --- e2e: the same solve with pinned host buffers through the C ABI ----
+    bh = [torch.from_numpy(W.b[D.ranges[q]:D.ranges[q + 1]].copy()).pin_memory().numpy()
+          for q in range(P)]
+    xh = [torch.zeros(cm.vec_len(q), dtype=torch.float64).pin_memory().numpy()
+          for q in range(P)]
+    S.cg(comm, M, bh, 10000, W.rtol, x=xh)
+    barrier(world, device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        S.cg(comm, M, bh, 10000, W.rtol, x=xh)
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    barrier(world, device)
+    te = max_over_ranks(e0.elapsed_time(e1) / 1e3, world, device)
+    e2e = world * args.steps / te
+    h2d = int(sum(v.nbytes for v in bh))
+    d2h = int(sum(D.local_sizes[q] * 8 for q in range(P)))
+
+    # --- roofline of the product kernel (matvec loop: update + mult) -------
+    xs = [torch.rand(cm.vec_len(q), dtype=torch.float64, device=f"cuda:{device}")
+          for q in range(P)]
+    ys = [torch.empty(D.local_sizes[q], dtype=torch.float64, device=f"cuda:{device}")
+          for q in range(P)]
+    reps = args.spmv_reps
+    for _ in range(5):
+        cm.update(xs)
+        M.mult(xs, out=ys)
+    barrier(world, device)
+    a0, a1, a2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    a0.record(stream)
+    for _ in range(reps):
+        M.mult(xs, out=ys)
+    a1.record(stream)
+    for _ in range(reps):
+        cm.update(xs)
+        M.mult(xs, out=ys)
+    a2.record(stream)
+    torch.cuda.synchronize(device)
+    t_mult = a0.elapsed_time(a1) / 1e3 / reps
+    t_pair = a1.elapsed_time(a2) / 1e3 / reps
+    hbm, src = peaks()
+    kb = kernel_bytes(n, nnz, P, g)
+    achieved = kb / t_mult / 1e9
+    sb = spmv_bytes(n, nnz, P, g)
+    traffic = None
+    tp = ROOT / "profiles" / "traffic.json"
+    if tp.exists():
+        try:
+            traffic = json.loads(tp.read_text()).get("spmv_vector_kernel_c2")
+        except Exception:
+            traffic = None
+
+    # CG iteration bytes (fused-halo layout: no ghost gather, 9 n vector terms).
+    b_iter = kernel_bytes(n, nnz, 1, 0) + 9 * n * 8
+    ms_per_iter = t_local / args.steps / k_mean * 1e3
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        import oracle
+        nth = oracle.max_threads()
+        spi, kk = cpu_sample(W, D, args.cpu_budget, nth)
+        cpu = {"value": 1.0 / (spi * k_mean), "unit": "solves/s", "cores": nth,
+               "kind": "port",
+               "sample": "oracle spmv::cg restatement on %d host threads: %d CG "
+                         "iterations timed (%.1f s), scaled to the %.0f iterations "
+                         "of a full solve" % (nth, kk, spi * kk, k_mean)}
+
+    if rank == 0:
+        line = {
+            "metric": "CG solves/s", "value": value, "unit": "solves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": config_dict(W, D, P),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_source": src, "traffic": traffic,
+                         "kernel": "spmv_vector_kernel (Matrix::mult, 8 ranks, one launch)",
+                         "bytes_per_launch": kb, "us_per_launch": t_mult * 1e6},
+            "spmv": {"update_plus_mult_gbs": sb / t_pair / 1e9,
+                     "update_plus_mult_us": t_pair * 1e6, "bytes": sb,
+                     "frac_of_measured_hbm": sb / t_pair / 1e9 / hbm,
+                     "frac_of_8TBs": sb / t_pair / 1e9 / 8000.0},
+            "cg": {"iterations": k_mean, "ms_per_iter": ms_per_iter,
+                   "gbs": b_iter / (ms_per_iter / 1e3) / 1e9,
+                   "bytes_per_iter": b_iter},
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(args.steps * (1 + 3 * k_mean)),
+            "clocks": clk,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--spmv-reps", type=int, default=200)
+    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--ref-budget", type=float, default=1.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,234 @@
+/*
+ * spmv_b200.h - C ABI of the B200 (sm_100a) implementation of libspmv's hot
+ * path: the distributed CSR product (spmv::Matrix), the ghost map and halo
+ * exchange (spmv::L2GMap) and conjugate gradients (spmv::cg).
+ *
+ * Conventions
+ *  - Every entry point returns an int status (SPMV_SUCCESS == 0).  On failure
+ *    spmv_last_error() returns the message of the calling thread's last error;
+ *    where the reference throws std::runtime_error, the message is the same
+ *    string (e.g. "Ghosts must be sorted", L2GMap.cpp:35).
+ *  - The reference is an MPI library: one rank holds one row block.  Here one
+ *    spmv_comm is a *virtual communicator* of `size` ranks that all live on one
+ *    GPU.  Calls that are collective in the reference (L2GMap construction,
+ *    update, reverse_update, cg) take the arrays of all ranks at once: an
+ *    argument declared `T const* x` with the comment "[size]" holds one entry
+ *    per rank, in rank order.
+ *  - Vectors are passed per rank as plain pointers.  With SPMV_MEMORY_HOST the
+ *    call copies them to the device, runs the kernels and copies results back
+ *    before returning.  With SPMV_MEMORY_DEVICE they are device pointers and
+ *    the call is ordered on the communicator's CUDA stream.
+ *  - The library owns device copies of matrices and maps; callers own every
+ *    buffer they pass in.  There is no CPU compute path: every product,
+ *    gather, scatter-add and solver step runs as a CUDA kernel.
+ */
+#ifndef SPMV_B200_H
+#define SPMV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPMV_B200_VERSION_MAJOR 0
+#define SPMV_B200_VERSION_MINOR 1
+
+/* Largest number of virtual ranks (row-block partitions) per communicator. */
+#define SPMV_MAX_PARTS 64
+
+typedef enum spmv_status {
+  SPMV_SUCCESS = 0,
+  SPMV_ERROR_INVALID_ARGUMENT = 1, /* bad sizes, unsorted ghosts, ...       */
+  SPMV_ERROR_CUDA = 2,             /* a CUDA runtime call failed           */
+  SPMV_ERROR_OUT_OF_MEMORY = 3,
+  SPMV_ERROR_NO_DEVICE = 4,        /* device work on a host-only comm      */
+  SPMV_ERROR_BREAKDOWN = 5,        /* CG: p.Ap is zero or not finite       */
+  SPMV_ERROR_NOT_SUPPORTED = 6,    /* dtype / option not implemented       */
+  SPMV_ERROR_INTERNAL = 7
+} spmv_status;
+
+/* Scalar type of a matrix or vector; replaces spmv::mpi_type<T>()
+ * (mpi_type.h:11-33). */
+typedef enum spmv_dtype {
+  SPMV_FLOAT64 = 0,
+  SPMV_FLOAT32 = 1,
+  SPMV_COMPLEX64 = 2,  /* std::complex<float>  (not yet implemented) */
+  SPMV_COMPLEX128 = 3  /* std::complex<double> (not yet implemented) */
+} spmv_dtype;
+
+typedef enum spmv_memory {
+  SPMV_MEMORY_HOST = 0,
+  SPMV_MEMORY_DEVICE = 1
+} spmv_memory;
+
+/* SpMV kernel family used by a matrix (see spmv_matrix_set_kernel). */
+typedef enum spmv_kernel {
+  SPMV_KERNEL_AUTO = 0,   /* chosen from row-length statistics          */
+  SPMV_KERNEL_VECTOR = 1, /* vector CSR: a W-lane group per row          */
+  SPMV_KERNEL_MERGE = 2   /* merge-path, load balanced for skewed rows   */
+} spmv_kernel;
+
+/* Fields of the communication pattern of one rank of an L2GMap.  They are
+ * the members of the same names in the reference (L2GMap.h:80-91). */
+typedef enum spmv_pattern_field {
+  SPMV_PATTERN_NEIGHBOURS = 0,
+  SPMV_PATTERN_SEND_COUNT = 1,
+  SPMV_PATTERN_RECV_COUNT = 2,
+  SPMV_PATTERN_SEND_OFFSET = 3,
+  SPMV_PATTERN_RECV_OFFSET = 4,
+  SPMV_PATTERN_INDEXBUF = 5
+} spmv_pattern_field;
+
+typedef struct spmv_comm_s* spmv_comm;
+typedef struct spmv_l2gmap_s* spmv_l2gmap;
+typedef struct spmv_matrix_s* spmv_matrix;
+
+/* ------------------------------------------------------------------------ */
+/* Errors and version                                                        */
+/* ------------------------------------------------------------------------ */
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* spmv_last_error(void);
+int spmv_get_version(int* major, int* minor);
+
+/* ------------------------------------------------------------------------ */
+/* Virtual communicator.  Replaces the MPI_Comm argument of the reference    */
+/* (L2GMap.h:29, Matrix.h:59, cg.h:27).                                      */
+/* ------------------------------------------------------------------------ */
+
+/* device >= 0: ranks live on that CUDA device; `stream` is a cudaStream_t to
+ * order work on (NULL: the library creates its own non-blocking stream).
+ * device == -1: a host-only communicator; maps and matrices can be built and
+ * inspected, device work fails with SPMV_ERROR_NO_DEVICE. */
+int spmv_comm_create(int device, void* stream, int size, spmv_comm* comm);
+int spmv_comm_destroy(spmv_comm comm);
+int spmv_comm_size(spmv_comm comm, int* size);
+int spmv_comm_device(spmv_comm comm, int* device);
+int spmv_comm_stream(spmv_comm comm, void** stream);
+int spmv_comm_synchronize(spmv_comm comm);
+
+/* ------------------------------------------------------------------------ */
+/* L2GMap (reference: L2GMap.h:14-97, L2GMap.cpp:15-199)                     */
+/* ------------------------------------------------------------------------ */
+
+/* Collective construction (L2GMap::L2GMap, L2GMap.cpp:15-122) for all ranks:
+ * local_size[size], ghosts[size][num_ghosts[r]] (global indices, sorted
+ * ascending, none in the rank's own range).  Errors: "Ghosts must be sorted"
+ * (L2GMap.cpp:35), "Ghost index in local range" (L2GMap.cpp:45). */
+int spmv_l2gmap_create(spmv_comm comm, const int64_t* local_size,
+                       const int64_t* const* ghosts, const int64_t* num_ghosts,
+                       spmv_l2gmap* map);
+int spmv_l2gmap_destroy(spmv_l2gmap map);
+/* L2GMap::local_size, num_ghosts, global_size, global_offset
+ * (L2GMap.cpp:187-199). */
+int spmv_l2gmap_local_size(spmv_l2gmap map, int rank, int32_t* out);
+int spmv_l2gmap_num_ghosts(spmv_l2gmap map, int rank, int32_t* out);
+int spmv_l2gmap_global_size(spmv_l2gmap map, int64_t* out);
+int spmv_l2gmap_global_offset(spmv_l2gmap map, int rank, int64_t* out);
+/* L2GMap::global_to_local (L2GMap.cpp:172-185).  An index neither owned by
+ * nor ghosted on `rank` is an error (the reference's behaviour there is
+ * undefined). */
+int spmv_l2gmap_global_to_local(spmv_l2gmap map, int rank,
+                                int64_t global_index, int32_t* out);
+/* L2GMap::ghosts (L2GMap.h:75).  *ghosts stays valid while the map lives. */
+int spmv_l2gmap_ghosts(spmv_l2gmap map, int rank, const int64_t** ghosts,
+                       int32_t* n);
+/* One array of the rank's communication pattern (L2GMap.h:80-91), exactly as
+ * the reference computes it, including send_offset already shifted by
+ * local_size (L2GMap.cpp:120-121).  *data stays valid while the map lives. */
+int spmv_l2gmap_pattern(spmv_l2gmap map, int rank, spmv_pattern_field field,
+                        const int32_t** data, int32_t* n);
+/* L2GMap::update<T> (L2GMap.cpp:126-150): for all ranks at once, copy each
+ * owner's values into the ghost slots of the ranks that ghost them.
+ * vecs[size], each of length local_size + num_ghosts.  Bit-exact copy. */
+int spmv_l2gmap_update(spmv_l2gmap map, spmv_dtype dtype, spmv_memory memory,
+                       void* const* vecs);
+/* L2GMap::reverse_update<T> (L2GMap.cpp:152-170): add every ghost slot into
+ * its owner's entry, in the reference's order (neighbour rank order, then
+ * ghost order), so results are bitwise those of the reference loop. */
+int spmv_l2gmap_reverse_update(spmv_l2gmap map, spmv_dtype dtype,
+                               spmv_memory memory, void* const* vecs);
+
+/* ------------------------------------------------------------------------ */
+/* Matrix (reference: Matrix.h:23-81, Matrix.cpp:13-211)                     */
+/* ------------------------------------------------------------------------ */
+
+/* Matrix::Matrix (Matrix.cpp:13-22) plus the inspector step mkl_init
+ * (Matrix.cpp:34-51): copies in every rank's local CSR block (0-based,
+ * int32 row pointers and column indices, columns [0, ncols) with the
+ * col_map's ghosts after its owned range).  nrows[size], ncols[size],
+ * rowptr[size][nrows[r]+1], colind[size][nnz], values[size][nnz] of `dtype`.
+ * row_map may be NULL (then rows have no map, and spmv_cg is refused). */
+int spmv_matrix_create_csr(spmv_comm comm, spmv_dtype dtype,
+                           spmv_l2gmap col_map, spmv_l2gmap row_map,
+                           const int32_t* nrows, const int32_t* ncols,
+                           const int32_t* const* rowptr,
+                           const int32_t* const* colind,
+                           const void* const* values, spmv_matrix* A);
+int spmv_matrix_destroy(spmv_matrix A);
+/* Matrix::operator* (Matrix.cpp:158-166, 199-204): y[r] = A[r] x[r] for all
+ * ranks in one launch.  x[r] has ncols[r] entries (owned, then ghosts: run
+ * spmv_l2gmap_update first, as the reference's callers do), y[r] nrows[r]. */
+int spmv_matrix_mult(spmv_matrix A, spmv_memory memory, const void* const* x,
+                     void* const* y);
+/* Matrix::transpmult (Matrix.cpp:168-176, 206-211): y[r] = A[r]^T x[r];
+ * x[r] has nrows[r] entries, y[r] ncols[r] (ghost tail included: follow with
+ * spmv_l2gmap_reverse_update, as restrictmain.cpp:60-66 does). */
+int spmv_matrix_transpmult(spmv_matrix A, spmv_memory memory,
+                           const void* const* x, void* const* y);
+int spmv_matrix_dtype(spmv_matrix A, spmv_dtype* dtype);
+int spmv_matrix_rows(spmv_matrix A, int rank, int32_t* nrows);
+int spmv_matrix_cols(spmv_matrix A, int rank, int32_t* ncols);
+int spmv_matrix_nnz(spmv_matrix A, int rank, int64_t* nnz);
+/* Matrix::mat() (Matrix.h:51-53): the host copy of rank's CSR block. */
+int spmv_matrix_csr(spmv_matrix A, int rank, const int32_t** rowptr,
+                    const int32_t** colind, const void** values);
+/* Matrix::col_map()/row_map() (Matrix.h:45-48). */
+int spmv_matrix_col_map(spmv_matrix A, spmv_l2gmap* map);
+int spmv_matrix_row_map(spmv_matrix A, spmv_l2gmap* map);
+/* Replace the values of every rank (same sparsity pattern).  values[size]. */
+int spmv_matrix_set_values(spmv_matrix A, spmv_memory memory,
+                           const void* const* values);
+/* Kernel choice.  width: lanes per row for SPMV_KERNEL_VECTOR (1..32, power
+ * of two; 0 = from statistics); block: threads per CTA (0 = default). */
+int spmv_matrix_set_kernel(spmv_matrix A, spmv_kernel kernel, int width,
+                           int block);
+int spmv_matrix_get_kernel(spmv_matrix A, spmv_kernel* kernel, int* width,
+                           int* block);
+
+/* ------------------------------------------------------------------------ */
+/* Conjugate gradients (reference: cg.h:27-29, cg.cpp:11-83)                 */
+/* ------------------------------------------------------------------------ */
+
+typedef struct spmv_cg_info {
+  int iterations;          /* k as returned by spmv::cg                    */
+  int status;              /* SPMV_SUCCESS or SPMV_ERROR_BREAKDOWN          */
+  double rnorm0;           /* ||b||^2                                       */
+  double rnorm;            /* last recursive ||r||^2                        */
+} spmv_cg_info;
+
+/* spmv::cg (cg.cpp:11-83): unpreconditioned CG from x0 = 0 on all ranks at
+ * once, stopping when ||r||^2/||b||^2 < rtol^2 or after max_its iterations.
+ * b[size] (row_map local_size entries each; b_rows[size] gives their lengths
+ * for the "b.rows() != A.rows()" check, or NULL to skip it), x[size] out
+ * (col_map local_size + num_ghosts entries each; the ghost tail is zero, as
+ * in the reference).  FP64 only.  Each iteration runs as one CUDA graph body
+ * under a device-side while loop; there is no host round trip per iteration.
+ * Differences from the reference: b == 0 returns x = 0 after 0 iterations
+ * (the reference divides 0 by 0), and p.Ap == 0 or non-finite stops with
+ * SPMV_ERROR_BREAKDOWN (the reference carries NaN to max_its). */
+int spmv_cg(spmv_matrix A, spmv_memory memory, const double* const* b,
+            const int64_t* b_rows, double* const* x, int max_its, double rtol,
+            int* num_its);
+/* As spmv_cg, filling *info (may be NULL). */
+int spmv_cg_ex(spmv_matrix A, spmv_memory memory, const double* const* b,
+               const int64_t* b_rows, double* const* x, int max_its,
+               double rtol, spmv_cg_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPMV_B200_H */

@@ -1,0 +1,162 @@
+"""ORACLE - TEST INFRASTRUCTURE ONLY.
+
+Python access to the CPU restatement of libspmv's hot path (oracle.cpp),
+plus the recipe that builds it.  Only the tests, the smoke check and the
+CPU-baseline leg of bench.py may use this package; the product never does.
+Parity is unpinned: the reference cannot be built here and ships no golden
+outputs (see oracle.cpp's header).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+from typing import List, Sequence
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle_spmv.so"
+_lib = None
+
+
+def build(force: bool = False) -> Path:
+    src = HERE / "oracle.cpp"
+    if force or not LIB_PATH.exists() or src.stat().st_mtime > LIB_PATH.stat().st_mtime:
+        subprocess.run(["make", "-C", str(HERE), "-B" if force else "-s"], check=True,
+                       capture_output=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: run `make -C oracle`")
+        L = C.CDLL(str(LIB_PATH))
+        P, I32, I64, D = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+        L.oracle_last_error.restype = C.c_char_p
+        L.oracle_owner_ranges.argtypes = [I64, I64, P]
+        L.oracle_map_create.argtypes = [C.c_int, P, P, P, C.POINTER(P)]
+        L.oracle_map_free.argtypes = [P]
+        L.oracle_map_field.argtypes = [P, C.c_int, C.c_int,
+                                       C.POINTER(C.POINTER(I32)), C.POINTER(I32)]
+        L.oracle_map_global_to_local.argtypes = [P, C.c_int, I64]
+        L.oracle_map_global_to_local.restype = I32
+        for n in ("oracle_update_f64", "oracle_update_f32", "oracle_reverse_update_f64",
+                  "oracle_reverse_update_f32"):
+            getattr(L, n).argtypes = [P, P]
+        L.oracle_csr_mult_f64.argtypes = [I32, P, P, P, P, P, C.c_int]
+        L.oracle_csr_mult_f32.argtypes = [I32, P, P, P, P, P]
+        L.oracle_csr_transpmult_f64.argtypes = [I32, I32, P, P, P, P, P]
+        L.oracle_csr_transpmult_f32.argtypes = [I32, I32, P, P, P, P, P]
+        L.oracle_cg.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_int, D, C.c_int,
+                                C.c_int, C.POINTER(D)]
+        L.oracle_cg.restype = C.c_int
+        L.oracle_matvec_demo.argtypes = [C.c_int, I64, C.c_int]
+        L.oracle_matvec_demo.restype = D
+        L.oracle_max_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _parr(arrs):
+    out = (C.c_void_p * max(1, len(arrs)))()
+    for i, a in enumerate(arrs):
+        out[i] = a.ctypes.data
+    return out
+
+
+def owner_ranges(size: int, N: int) -> np.ndarray:
+    out = np.zeros(size + 1, np.int64)
+    lib().oracle_owner_ranges(size, N, out.ctypes.data)
+    return out
+
+
+class Map:
+    """The reference's L2GMap for all ranks (L2GMap.cpp:15-122 restated)."""
+
+    def __init__(self, local_sizes: Sequence[int], ghosts: Sequence[np.ndarray]):
+        self.P = len(local_sizes)
+        self._ls = np.asarray(local_sizes, np.int64)
+        self._g = [np.ascontiguousarray(g, np.int64) for g in ghosts]
+        self._ng = np.array([len(g) for g in self._g], np.int64)
+        h = C.c_void_p()
+        if lib().oracle_map_create(self.P, self._ls.ctypes.data, _parr(self._g),
+                                   self._ng.ctypes.data, C.byref(h)) != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        self._h = h
+
+    def field(self, rank: int, name: str) -> np.ndarray:
+        idx = {"neighbours": 0, "send_count": 1, "recv_count": 2, "send_offset": 3,
+               "recv_offset": 4, "indexbuf": 5}[name]
+        p, n = C.POINTER(C.c_int32)(), C.c_int32()
+        if lib().oracle_map_field(self._h, rank, idx, C.byref(p), C.byref(n)) != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return np.ctypeslib.as_array(p, (n.value,)).copy() if n.value else \
+            np.zeros(0, np.int32)
+
+    def global_to_local(self, rank: int, i: int) -> int:
+        return lib().oracle_map_global_to_local(self._h, rank, i)
+
+    def update(self, vecs: List[np.ndarray]) -> None:
+        f = lib().oracle_update_f64 if vecs[0].dtype == np.float64 else lib().oracle_update_f32
+        f(self._h, _parr(vecs))
+
+    def reverse_update(self, vecs: List[np.ndarray]) -> None:
+        f = (lib().oracle_reverse_update_f64 if vecs[0].dtype == np.float64
+             else lib().oracle_reverse_update_f32)
+        f(self._h, _parr(vecs))
+
+    def __del__(self):
+        try:
+            lib().oracle_map_free(self._h)
+        except Exception:
+            pass
+
+
+def csr_mult(rp, ci, v, x, nthreads: int = 1) -> np.ndarray:
+    m = len(rp) - 1
+    y = np.empty(m, v.dtype)
+    if v.dtype == np.float64:
+        lib().oracle_csr_mult_f64(m, rp.ctypes.data, ci.ctypes.data, v.ctypes.data,
+                                  x.ctypes.data, y.ctypes.data, nthreads)
+    else:
+        lib().oracle_csr_mult_f32(m, rp.ctypes.data, ci.ctypes.data, v.ctypes.data,
+                                  x.ctypes.data, y.ctypes.data)
+    return y
+
+
+def csr_transpmult(rp, ci, v, x, ncols: int) -> np.ndarray:
+    m = len(rp) - 1
+    y = np.empty(ncols, v.dtype)
+    f = (lib().oracle_csr_transpmult_f64 if v.dtype == np.float64
+         else lib().oracle_csr_transpmult_f32)
+    f(m, ncols, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, x.ctypes.data,
+      y.ctypes.data)
+    return y
+
+
+def cg(col_map: Map, blocks, b: List[np.ndarray], max_its: int, rtol: float,
+       nthreads: int = 1, max_its_run: int | None = None):
+    """spmv::cg (cg.cpp:11-83) restated; returns (x per rank, k, rnorm)."""
+    P = col_map.P
+    nrows = np.array([len(blk[0]) - 1 for blk in blocks], np.int32)
+    rps = [np.ascontiguousarray(blk[0], np.int32) for blk in blocks]
+    cis = [np.ascontiguousarray(blk[1], np.int32) for blk in blocks]
+    vas = [np.ascontiguousarray(blk[2], np.float64) for blk in blocks]
+    bs = [np.ascontiguousarray(v, np.float64) for v in b]
+    xs = [np.zeros(col_map._ls[q] + col_map._ng[q]) for q in range(P)]
+    rn = C.c_double()
+    k = lib().oracle_cg(col_map._h, P, nrows.ctypes.data, _parr(rps), _parr(cis),
+                        _parr(vas), _parr(bs), _parr(xs), max_its, rtol, nthreads,
+                        max_its if max_its_run is None else max_its_run, C.byref(rn))
+    return xs, k, rn.value
+
+
+def matvec_demo(P: int, N: int = 500000, n_apply: int = 1000) -> float:
+    return lib().oracle_matvec_demo(P, N, n_apply)
+
+
+def max_threads() -> int:
+    return lib().oracle_max_threads()

@@ -1,0 +1,511 @@
+// ORACLE - TEST INFRASTRUCTURE ONLY.
+//
+// A CPU restatement of libspmv's hot path (chrisrichardson/spmv), used to
+// check the CUDA implementation.  Only the tests, the smoke check and the
+// CPU-baseline leg of bench.py load this library; the product never does.
+//
+// Parity is UNPINNED: the reference cannot be built here (it needs Eigen,
+// MKL or BLAS, and MPI, none of which are installed) and it ships no tests,
+// fixtures or golden outputs.  Each function below restates the reference's
+// code at the cited file:line; results are cross-checked against
+// scipy.sparse in the tests, which is independent evidence but not a pin.
+//
+// MPI is replaced by a virtual communicator: all P ranks' data is in this
+// process, and each collective is restated by its MPI semantics (who sends
+// which block to whom), not by a shortcut, so the arrays it produces are the
+// ones each MPI rank would hold.
+//
+// Floating point: the reference is built with -O3 and no -march (x86-64
+// baseline, no FMA); this file is built with -ffp-contract=off so products
+// and sums round separately, as they do there.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+thread_local std::string g_err;
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// L2GMap restated (L2GMap.cpp:15-122) over a virtual communicator.
+// ---------------------------------------------------------------------------
+struct Rank {
+  int64_t local_size = 0;
+  std::vector<int64_t> ghosts;
+  std::map<int64_t, int32_t> global_to_local;   // L2GMap.h:76
+  std::vector<int> neighbours;
+  std::vector<int32_t> ghost_local, send_count, recv_count, send_offset,
+      recv_offset, indexbuf;
+};
+
+struct Map {
+  int P = 0;
+  std::vector<int64_t> ranges;
+  std::vector<Rank> r;
+};
+
+// Position of rank `who` in rank `at`'s neighbour list (the dist-graph
+// communicator of L2GMap.cpp:81-84 has sources == destinations ==
+// neighbours, in that order).
+int position(const Map& m, int at, int who) {
+  const auto& nb = m.r[at].neighbours;
+  auto it = std::find(nb.begin(), nb.end(), who);
+  if (it == nb.end()) throw std::runtime_error("oracle: asymmetric neighbours");
+  return int(it - nb.begin());
+}
+
+void build_map(Map& m, int P, const int64_t* local_size,
+               const int64_t* const* ghosts, const int64_t* nghosts) {
+  m.P = P;
+  m.r.assign(P, Rank{});
+  // MPI_Allgather of local_size, then prefix sum (L2GMap.cpp:23-28).
+  m.ranges.assign(P + 1, 0);
+  for (int q = 0; q < P; ++q) m.ranges[q + 1] = local_size[q];
+  for (int i = 0; i < P; ++i) m.ranges[i + 1] += m.ranges[i];
+
+  std::vector<std::vector<int32_t>> ghost_count(P, std::vector<int32_t>(P, 0));
+  for (int rank = 0; rank < P; ++rank) {
+    Rank& R = m.r[rank];
+    R.local_size = local_size[rank];
+    R.ghosts.assign(ghosts[rank], ghosts[rank] + nghosts[rank]);
+    const int64_t r0 = m.ranges[rank], r1 = m.ranges[rank + 1];
+    if (!std::is_sorted(R.ghosts.begin(), R.ghosts.end()))   // :34-35
+      throw std::runtime_error("Ghosts must be sorted");
+    for (size_t i = 0; i < R.ghosts.size(); ++i) {            // :40-54
+      const int64_t idx = R.ghosts[i];
+      if (idx >= r0 and idx < r1)
+        throw std::runtime_error("Ghost index in local range");
+      R.global_to_local.insert({idx, int32_t(R.local_size + int64_t(i))});
+      auto it = std::upper_bound(m.ranges.begin(), m.ranges.end(), idx);
+      const int p = int(it - m.ranges.begin()) - 1;
+      ++ghost_count[rank][p];
+      R.ghost_local.push_back(int32_t(R.ghosts[i] - m.ranges[p]));
+    }
+  }
+  // MPI_Alltoall: remote_count[rank][i] = ghost_count[i][rank] (:59-61);
+  // neighbour lists and send counts (:63-78).
+  for (int rank = 0; rank < P; ++rank) {
+    Rank& R = m.r[rank];
+    for (int i = 0; i < P; ++i) {
+      const int32_t c = ghost_count[rank][i];
+      const int32_t rc = ghost_count[i][rank];
+      if (c > 0) {
+        R.neighbours.push_back(i);
+        R.send_count.push_back(c);
+      } else if (rc > 0) {
+        R.neighbours.push_back(i);
+        R.send_count.push_back(0);
+      }
+    }
+    R.recv_count.assign(R.neighbours.size(), 0);            // :86
+    if (R.neighbours.empty()) {                              // :87-92
+      R.send_count = {0};
+      R.recv_count = {0};
+    }
+  }
+  // MPI_Neighbor_alltoall of send_count (:97-98): block k of rank `rank`
+  // comes from neighbour q = neighbours[k], which sends its block for
+  // `rank` (at rank's position in q's list).
+  for (int rank = 0; rank < P; ++rank) {
+    Rank& R = m.r[rank];
+    for (size_t k = 0; k < R.neighbours.size(); ++k) {
+      const int q = R.neighbours[k];
+      R.recv_count[k] = m.r[q].send_count[position(m, q, rank)];
+    }
+  }
+  for (int rank = 0; rank < P; ++rank) {                     // :100-109
+    Rank& R = m.r[rank];
+    R.send_offset = {0};
+    for (int c : R.send_count) R.send_offset.push_back(R.send_offset.back() + c);
+    R.recv_offset = {0};
+    for (int c : R.recv_count) R.recv_offset.push_back(R.recv_offset.back() + c);
+    R.indexbuf.assign(R.recv_offset.back(), 0);
+  }
+  // MPI_Neighbor_alltoallv of ghost_local (:112-115).
+  for (int rank = 0; rank < P; ++rank) {
+    Rank& R = m.r[rank];
+    for (size_t k = 0; k < R.neighbours.size(); ++k) {
+      const int q = R.neighbours[k];
+      const int pos = position(m, q, rank);
+      const Rank& Q = m.r[q];
+      for (int32_t j = 0; j < R.recv_count[k]; ++j)
+        R.indexbuf[R.recv_offset[k] + j] = Q.ghost_local[Q.send_offset[pos] + j];
+    }
+  }
+  for (int rank = 0; rank < P; ++rank)                       // :120-121
+    for (int32_t& s : m.r[rank].send_offset) s += int32_t(m.r[rank].local_size);
+}
+
+// L2GMap::update<T> (L2GMap.cpp:126-150).  Every rank packs databuf from its
+// own vector first; then the alltoallv delivers rank q's segment for `rank`
+// (recv_count/offset on the sender side, send_count/offset on the receiver
+// side: the meanings are reversed, L2GMap.cpp:141-147).
+template <typename T>
+void update(const Map& m, T* const* vec) {
+  std::vector<std::vector<T>> databuf(m.P);
+  for (int rank = 0; rank < m.P; ++rank) {
+    const Rank& R = m.r[rank];
+    databuf[rank].resize(R.indexbuf.size());
+    for (size_t i = 0; i < R.indexbuf.size(); ++i)
+      databuf[rank][i] = vec[rank][R.indexbuf[i]];
+  }
+  for (int rank = 0; rank < m.P; ++rank) {
+    const Rank& R = m.r[rank];
+    for (size_t k = 0; k < R.neighbours.size(); ++k) {
+      const int q = R.neighbours[k];
+      const int pos = position(m, q, rank);
+      const Rank& Q = m.r[q];
+      for (int32_t j = 0; j < R.send_count[k]; ++j)
+        vec[rank][R.send_offset[k] + j] = databuf[q][Q.recv_offset[pos] + j];
+    }
+  }
+}
+
+// L2GMap::reverse_update<T> (L2GMap.cpp:152-170).
+template <typename T>
+void reverse_update(const Map& m, T* const* vec) {
+  std::vector<std::vector<T>> databuf(m.P);
+  for (int rank = 0; rank < m.P; ++rank) {
+    const Rank& R = m.r[rank];
+    databuf[rank].assign(R.indexbuf.size(), T(0));
+    for (size_t k = 0; k < R.neighbours.size(); ++k) {
+      const int q = R.neighbours[k];
+      const int pos = position(m, q, rank);
+      const Rank& Q = m.r[q];
+      for (int32_t j = 0; j < R.recv_count[k]; ++j)
+        databuf[rank][R.recv_offset[k] + j] = vec[q][Q.send_offset[pos] + j];
+    }
+  }
+  for (int rank = 0; rank < m.P; ++rank) {
+    const Rank& R = m.r[rank];
+    for (size_t i = 0; i < R.indexbuf.size(); ++i)
+      vec[rank][R.indexbuf[i]] += databuf[rank][i];
+  }
+}
+
+// Matrix::operator* through Eigen's row-major sparse x dense product
+// (Matrix.cpp:199-204): per row, tmp = 0; tmp += v * x[c] in storage order.
+template <typename T>
+void csr_mult(int32_t m, const int32_t* rp, const int32_t* ci, const T* v,
+              const T* x, T* y, int nthreads) {
+  (void)nthreads;
+#pragma omp parallel for schedule(static) num_threads(nthreads) if (nthreads > 1)
+  for (int32_t i = 0; i < m; ++i) {
+    T tmp = T(0);
+    for (int32_t j = rp[i]; j < rp[i + 1]; ++j) tmp += v[j] * x[ci[j]];
+    y[i] = tmp;
+  }
+}
+
+// Matrix::transpmult (Matrix.cpp:206-211): Eigen's transposed product
+// scatters row by row: y = 0; y[c] += v * x[i].
+template <typename T>
+void csr_transpmult(int32_t m, int32_t n, const int32_t* rp, const int32_t* ci,
+                    const T* v, const T* x, T* y) {
+  std::fill(y, y + n, T(0));
+  for (int32_t i = 0; i < m; ++i)
+    for (int32_t j = rp[i]; j < rp[i + 1]; ++j) y[ci[j]] += v[j] * x[i];
+}
+
+double dot(const double* a, const double* b, int64_t n, int nthreads) {
+  if (nthreads <= 1) {
+    double s = 0.0;
+    for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+  }
+  // Parallel form (CPU baseline only): fixed chunks summed in chunk order.
+  const int64_t chunks = 256;
+  std::vector<double> part(chunks, 0.0);
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+  for (int64_t c = 0; c < chunks; ++c) {
+    const int64_t lo = n * c / chunks, hi = n * (c + 1) / chunks;
+    double s = 0.0;
+    for (int64_t i = lo; i < hi; ++i) s += a[i] * b[i];
+    part[c] = s;
+  }
+  double s = 0.0;
+  for (double p : part) s += p;
+  return s;
+}
+
+struct Mat {
+  std::vector<int32_t> nrows, ncols;
+  std::vector<const int32_t*> rp, ci;
+  std::vector<const double*> v;
+};
+
+}  // namespace
+
+extern "C" {
+
+typedef struct OracleMap* oracle_map;
+struct OracleMap {
+  Map m;
+};
+
+const char* oracle_last_error(void) { return g_err.c_str(); }
+
+// owner_ranges (CreateA.cpp:12-29, read_petsc.cpp:13-30): the first N % size
+// ranks get one extra row.
+void oracle_owner_ranges(int64_t size, int64_t N, int64_t* ranges) {
+  const int64_t n = N / size;
+  const int64_t r = N % size;
+  for (int64_t rank = 0; rank < size + 1; ++rank)
+    ranges[rank] = rank < r ? rank * (n + 1) : rank * n + r;
+}
+
+int oracle_map_create(int P, const int64_t* local_size,
+                      const int64_t* const* ghosts, const int64_t* nghosts,
+                      oracle_map* out) {
+  return guard([&] {
+    auto h = std::make_unique<OracleMap>();
+    build_map(h->m, P, local_size, ghosts, nghosts);
+    *out = h.release();
+  });
+}
+
+void oracle_map_free(oracle_map h) { delete h; }
+
+// field: 0 neighbours, 1 send_count, 2 recv_count, 3 send_offset,
+// 4 recv_offset, 5 indexbuf (same numbering as spmv_pattern_field).
+int oracle_map_field(oracle_map h, int rank, int field, const int32_t** data,
+                     int32_t* n) {
+  return guard([&] {
+    const Rank& R = h->m.r.at(rank);
+    static thread_local std::vector<int32_t> nb;
+    switch (field) {
+      case 0:
+        nb.assign(R.neighbours.begin(), R.neighbours.end());
+        *data = nb.data();
+        *n = int32_t(nb.size());
+        return;
+      case 1: *data = R.send_count.data(); *n = int32_t(R.send_count.size()); return;
+      case 2: *data = R.recv_count.data(); *n = int32_t(R.recv_count.size()); return;
+      case 3: *data = R.send_offset.data(); *n = int32_t(R.send_offset.size()); return;
+      case 4: *data = R.recv_offset.data(); *n = int32_t(R.recv_offset.size()); return;
+      case 5: *data = R.indexbuf.data(); *n = int32_t(R.indexbuf.size()); return;
+    }
+    throw std::runtime_error("oracle: bad field");
+  });
+}
+
+// L2GMap::global_to_local (L2GMap.cpp:172-185); -1 where the reference would
+// dereference map::end().
+int32_t oracle_map_global_to_local(oracle_map h, int rank, int64_t i) {
+  const Map& m = h->m;
+  const int64_t r0 = m.ranges[rank], r1 = m.ranges[rank + 1];
+  if (i >= r0 and i < r1) return int32_t(i - r0);
+  auto it = m.r[rank].global_to_local.find(i);
+  return it == m.r[rank].global_to_local.end() ? -1 : it->second;
+}
+
+void oracle_update_f64(oracle_map h, double* const* vec) { update<double>(h->m, vec); }
+void oracle_update_f32(oracle_map h, float* const* vec) { update<float>(h->m, vec); }
+void oracle_reverse_update_f64(oracle_map h, double* const* vec) {
+  reverse_update<double>(h->m, vec);
+}
+void oracle_reverse_update_f32(oracle_map h, float* const* vec) {
+  reverse_update<float>(h->m, vec);
+}
+
+void oracle_csr_mult_f64(int32_t m, const int32_t* rp, const int32_t* ci,
+                         const double* v, const double* x, double* y,
+                         int nthreads) {
+  csr_mult<double>(m, rp, ci, v, x, y, nthreads);
+}
+void oracle_csr_mult_f32(int32_t m, const int32_t* rp, const int32_t* ci,
+                         const float* v, const float* x, float* y) {
+  csr_mult<float>(m, rp, ci, v, x, y, 1);
+}
+void oracle_csr_transpmult_f64(int32_t m, int32_t n, const int32_t* rp,
+                               const int32_t* ci, const double* v,
+                               const double* x, double* y) {
+  csr_transpmult<double>(m, n, rp, ci, v, x, y);
+}
+void oracle_csr_transpmult_f32(int32_t m, int32_t n, const int32_t* rp,
+                               const int32_t* ci, const float* v,
+                               const float* x, float* y) {
+  csr_transpmult<float>(m, n, rp, ci, v, x, y);
+}
+
+// spmv::cg (cg.cpp:11-83) on all ranks.  The row map is assumed ghost-free
+// and b[rank] has local_size entries; x[rank] receives local_size +
+// num_ghosts entries (ghost tail zero).  MPI_Allreduce(SUM) is the sum of
+// the ranks' values in rank order.  Returns the iteration count k.
+// nthreads > 1 parallelises products and dots (CPU baseline timing only).
+// max_its_run < max_its stops early after max_its_run iterations (a bounded
+// CPU sample); pass max_its_run = max_its for the full algorithm.
+int oracle_cg(oracle_map col_map, int P, const int32_t* nrows,
+              const int32_t* const* rp, const int32_t* const* ci,
+              const double* const* v, const double* const* b, double* const* x,
+              int kmax, double rtol, int nthreads, int max_its_run,
+              double* rnorm_out) {
+  const Map& cm = col_map->m;
+  std::vector<std::vector<double>> r(P), y(P), p(P);
+  std::vector<double*> pp(P);
+  for (int q = 0; q < P; ++q) {
+    const int M = nrows[q];
+    const int64_t L = cm.r[q].local_size + int64_t(cm.r[q].ghosts.size());
+    r[q].assign(b[q], b[q] + M);                        // r = b
+    y[q].assign(M, 0.0);
+    p[q].assign(L, 0.0);                                // p.setZero()
+    std::copy(r[q].begin(), r[q].end(), p[q].begin());  // p.head(M) = r
+    std::fill(x[q], x[q] + L, 0.0);                     // x.setZero()
+    pp[q] = p[q].data();
+  }
+  auto allreduce = [&](auto&& f) {
+    double s = 0.0;
+    for (int q = 0; q < P; ++q) s += f(q);
+    return s;
+  };
+  const double rnorm0 = allreduce([&](int q) {
+    return dot(r[q].data(), r[q].data(), nrows[q], nthreads);
+  });
+  const double rtol2 = rtol * rtol;
+  double rnorm_old = rnorm0;
+  int k = 0;
+  while (k < kmax && k < max_its_run) {
+    ++k;
+    update<double>(cm, pp.data());                      // col_l2g->update(p)
+    for (int q = 0; q < P; ++q)                         // y = A * p
+      csr_mult<double>(nrows[q], rp[q], ci[q], v[q], p[q].data(), y[q].data(),
+                       nthreads);
+    const double pdoty_sum = allreduce([&](int q) {
+      return dot(p[q].data(), y[q].data(), nrows[q], nthreads);
+    });
+    const double alpha = rnorm_old / pdoty_sum;
+    for (int q = 0; q < P; ++q) {
+      const int M = nrows[q];
+      for (int i = 0; i < M; ++i) x[q][i] += alpha * p[q][i];
+      for (int i = 0; i < M; ++i) r[q][i] -= alpha * y[q][i];
+    }
+    const double rnorm_new = allreduce([&](int q) {
+      return dot(r[q].data(), r[q].data(), nrows[q], nthreads);
+    });
+    const double beta = rnorm_new / rnorm_old;
+    rnorm_old = rnorm_new;
+    for (int q = 0; q < P; ++q)
+      for (int i = 0; i < nrows[q]; ++i) p[q][i] = p[q][i] * beta + r[q][i];
+    if (rnorm_new / rnorm0 < rtol2) break;
+  }
+  if (rnorm_out) *rnorm_out = rnorm_old;
+  return k;
+}
+
+// The matvec demo (matvecmain.cpp:16-121) on P virtual ranks: the operator of
+// create_A (CreateA.cpp:31-111) with N rows, psp[i] = exp(-10 (5 (z-0.5))^2),
+// z = global index / N, then n_apply times {update(psp); q = A psp;
+// psp.head(M) = q}.  Returns sum over ranks of ||psp.head(M)||^2.
+double oracle_matvec_demo(int P, int64_t N, int n_apply) {
+  std::vector<int64_t> ranges(P + 1);
+  oracle_owner_ranges(P, N, ranges.data());
+  // create_A: global-column tridiagonal rows, then ghosts and local columns.
+  std::vector<std::vector<int32_t>> rp(P), ci(P);
+  std::vector<std::vector<double>> va(P);
+  std::vector<int64_t> ls(P), ng(P);
+  std::vector<std::vector<int64_t>> gh(P);
+  const double gamma = 0.1;
+  for (int q = 0; q < P; ++q) {
+    const int64_t r0 = ranges[q], r1 = ranges[q + 1];
+    const int M = int(r1 - r0);
+    std::vector<std::vector<std::pair<int64_t, double>>> rows(M);
+    for (int i = 0; i < M; ++i) {
+      const int64_t c0 = r0 + i;
+      if (c0 == 0) {
+        rows[i] = {{c0, 1.0 - gamma}, {c0 + 1, gamma}};
+      } else if (c0 == N - 1) {
+        rows[i] = {{c0 - 1, gamma}, {c0, 1.0 - gamma}};
+      } else {
+        rows[i] = {{c0 - 1, gamma}, {c0, 1.0 - 2.0 * gamma}, {c0 + 1, gamma}};
+      }
+    }
+    std::vector<int64_t> g;
+    for (auto& row : rows)
+      for (auto& e : row)
+        if (e.first < r0 or e.first >= r1) g.push_back(e.first);
+    std::sort(g.begin(), g.end());
+    g.erase(std::unique(g.begin(), g.end()), g.end());
+    gh[q] = g;
+    ls[q] = M;
+    ng[q] = int64_t(g.size());
+    // Local columns (global_to_local) and setFromTriplets' sorted rows.
+    rp[q].assign(M + 1, 0);
+    for (int i = 0; i < M; ++i) {
+      std::vector<std::pair<int32_t, double>> loc;
+      for (auto& e : rows[i]) {
+        int32_t c;
+        if (e.first >= r0 && e.first < r1)
+          c = int32_t(e.first - r0);
+        else
+          c = int32_t(M + (std::lower_bound(g.begin(), g.end(), e.first) - g.begin()));
+        loc.push_back({c, e.second});
+      }
+      std::sort(loc.begin(), loc.end());
+      for (auto& e : loc) {
+        ci[q].push_back(e.first);
+        va[q].push_back(e.second);
+      }
+      rp[q][i + 1] = int32_t(ci[q].size());
+    }
+  }
+  std::vector<const int64_t*> gp(P);
+  for (int q = 0; q < P; ++q) gp[q] = gh[q].data();
+  Map m;
+  build_map(m, P, ls.data(), gp.data(), ng.data());
+  std::vector<std::vector<double>> psp(P), qv(P);
+  std::vector<double*> pp(P);
+  for (int q = 0; q < P; ++q) {
+    psp[q].assign(ls[q] + ng[q], 0.0);
+    for (int64_t i = 0; i < ls[q]; ++i) {
+      const double z = double(i + ranges[q]) / double(N);
+      psp[q][i] = std::exp(-10 * std::pow(5 * (z - 0.5), 2.0));
+    }
+    qv[q].assign(ls[q], 0.0);
+    pp[q] = psp[q].data();
+  }
+  for (int it = 0; it < n_apply; ++it) {
+    update<double>(m, pp.data());
+    for (int q = 0; q < P; ++q)
+      csr_mult<double>(int32_t(ls[q]), rp[q].data(), ci[q].data(), va[q].data(),
+                       psp[q].data(), qv[q].data(), 1);
+    for (int q = 0; q < P; ++q) std::copy(qv[q].begin(), qv[q].end(), psp[q].begin());
+  }
+  double s = 0.0;
+  for (int q = 0; q < P; ++q) {
+    double t = 0.0;
+    for (int64_t i = 0; i < ls[q]; ++i) t += psp[q][i] * psp[q][i];
+    s += t;
+  }
+  return s;
+}
+
+int oracle_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+}  // extern "C"

@@ -1,0 +1,331 @@
+"""Python mirror of libspmv's hot-path API over the C ABI.
+
+Names and argument meanings follow the reference (spmv::L2GMap, spmv::Matrix,
+spmv::cg); because the ranks of the reference's MPI communicator are virtual
+ranks on one GPU here, the collective calls take one entry per rank in lists.
+
+Vectors are numpy arrays (host memory: the call copies to the device and
+back) or CUDA torch tensors (device memory: used in place, ordered on the
+communicator's stream).  Errors raise SpmvError (a RuntimeError) carrying the
+reference's message where it has one.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import SpmvError, call, ptr_array
+
+_DTYPES = {np.dtype(np.float64): _lib.FLOAT64, np.dtype(np.float32): _lib.FLOAT32,
+           np.dtype(np.complex64): _lib.COMPLEX64,
+           np.dtype(np.complex128): _lib.COMPLEX128}
+_NP_OF = {v: k for k, v in _DTYPES.items()}
+
+
+def _is_torch(v) -> bool:
+    return type(v).__module__.startswith("torch")
+
+
+def _vec_info(vecs: Sequence):
+    """(memory kind, dtype code, addresses) of a per-rank vector list."""
+    if len(vecs) == 0:
+        raise SpmvError(_lib.ERROR_INVALID_ARGUMENT, "spmv: empty vector list")
+    kinds = {_is_torch(v) for v in vecs}
+    if len(kinds) != 1:
+        raise SpmvError(_lib.ERROR_INVALID_ARGUMENT,
+                        "spmv: mix of host and device vectors")
+    if kinds.pop():
+        import torch
+        for v in vecs:
+            if not v.is_cuda or not v.is_contiguous():
+                raise SpmvError(_lib.ERROR_INVALID_ARGUMENT,
+                                "spmv: device vectors must be contiguous CUDA tensors")
+        tdt = {torch.float64: _lib.FLOAT64, torch.float32: _lib.FLOAT32,
+               torch.complex64: _lib.COMPLEX64, torch.complex128: _lib.COMPLEX128}
+        dts = {tdt.get(v.dtype, -1) for v in vecs}
+        ptrs = [v.data_ptr() for v in vecs]
+        mem = _lib.MEMORY_DEVICE
+    else:
+        for v in vecs:
+            if not (isinstance(v, np.ndarray) and v.flags.c_contiguous):
+                raise SpmvError(_lib.ERROR_INVALID_ARGUMENT,
+                                "spmv: host vectors must be contiguous numpy arrays")
+        dts = {_DTYPES.get(v.dtype, -1) for v in vecs}
+        ptrs = [v.ctypes.data for v in vecs]
+        mem = _lib.MEMORY_HOST
+    if len(dts) != 1 or -1 in dts:
+        raise SpmvError(_lib.ERROR_INVALID_ARGUMENT,
+                        "spmv: vectors need one supported dtype")
+    return mem, dts.pop(), ptrs
+
+
+class Comm:
+    """Virtual communicator: `size` ranks on CUDA device `device` (-1 for a
+    host-only communicator that can build and inspect maps and matrices).
+    `stream` is a cudaStream_t handle (int) or None for a library stream."""
+
+    def __init__(self, size: int = 1, device: int = 0, stream: Optional[int] = None):
+        h = C.c_void_p()
+        call("spmv_comm_create", device, stream, size, C.byref(h))
+        self._h = h
+        self.size = size
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        call("spmv_comm_stream", self._h, C.byref(s))
+        return s.value or 0
+
+    def synchronize(self) -> None:
+        call("spmv_comm_synchronize", self._h)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.lib().spmv_comm_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class L2GMap:
+    """spmv::L2GMap (L2GMap.h:14-97) for every rank of `comm` at once:
+    local_sizes[r] owned entries and sorted ghost global indices ghosts[r]."""
+
+    def __init__(self, comm: Comm, local_sizes: Sequence[int],
+                 ghosts: Sequence[Sequence[int]]):
+        P = comm.size
+        if len(local_sizes) != P or len(ghosts) != P:
+            raise SpmvError(_lib.ERROR_INVALID_ARGUMENT,
+                            "spmv::L2GMap - Error: need one entry per rank")
+        self.comm = comm
+        ls = (C.c_int64 * P)(*[int(v) for v in local_sizes])
+        self._g = [np.ascontiguousarray(np.asarray(g, dtype=np.int64)) for g in ghosts]
+        gp = (C.POINTER(C.c_int64) * P)(
+            *[g.ctypes.data_as(C.POINTER(C.c_int64)) for g in self._g])
+        ng = (C.c_int64 * P)(*[len(g) for g in self._g])
+        h = C.c_void_p()
+        call("spmv_l2gmap_create", comm.handle, ls, gp, ng, C.byref(h))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def local_size(self, rank: int) -> int:
+        v = C.c_int32()
+        call("spmv_l2gmap_local_size", self._h, rank, C.byref(v))
+        return v.value
+
+    def num_ghosts(self, rank: int) -> int:
+        v = C.c_int32()
+        call("spmv_l2gmap_num_ghosts", self._h, rank, C.byref(v))
+        return v.value
+
+    def global_size(self) -> int:
+        v = C.c_int64()
+        call("spmv_l2gmap_global_size", self._h, C.byref(v))
+        return v.value
+
+    def global_offset(self, rank: int) -> int:
+        v = C.c_int64()
+        call("spmv_l2gmap_global_offset", self._h, rank, C.byref(v))
+        return v.value
+
+    def global_to_local(self, rank: int, i: int) -> int:
+        v = C.c_int32()
+        call("spmv_l2gmap_global_to_local", self._h, rank, int(i), C.byref(v))
+        return v.value
+
+    def ghosts(self, rank: int) -> np.ndarray:
+        p = C.POINTER(C.c_int64)()
+        n = C.c_int32()
+        call("spmv_l2gmap_ghosts", self._h, rank, C.byref(p), C.byref(n))
+        return np.ctypeslib.as_array(p, (n.value,)).copy() if n.value else \
+            np.zeros(0, np.int64)
+
+    def pattern(self, rank: int, field: str) -> np.ndarray:
+        p = C.POINTER(C.c_int32)()
+        n = C.c_int32()
+        call("spmv_l2gmap_pattern", self._h, rank, _lib.PATTERN_FIELDS[field],
+             C.byref(p), C.byref(n))
+        return np.ctypeslib.as_array(p, (n.value,)).copy() if n.value else \
+            np.zeros(0, np.int32)
+
+    def vec_len(self, rank: int) -> int:
+        return self.local_size(rank) + self.num_ghosts(rank)
+
+    def update(self, vecs: Sequence) -> None:
+        """L2GMap::update (L2GMap.cpp:126-150) on all ranks' vectors, in place."""
+        mem, dt, ptrs = _vec_info(vecs)
+        call("spmv_l2gmap_update", self._h, dt, mem, ptr_array(ptrs))
+
+    def reverse_update(self, vecs: Sequence) -> None:
+        """L2GMap::reverse_update (L2GMap.cpp:152-170), in place."""
+        mem, dt, ptrs = _vec_info(vecs)
+        call("spmv_l2gmap_reverse_update", self._h, dt, mem, ptr_array(ptrs))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.lib().spmv_l2gmap_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Matrix:
+    """spmv::Matrix<T> (Matrix.h:23-81): rank r's local CSR block
+    blocks[r] = (rowptr, colind, values) with columns numbered owned-then-
+    ghosts by col_map.  The block is copied in, as the reference's
+    constructor copies its Eigen matrix."""
+
+    def __init__(self, comm: Comm, blocks, col_map: Optional[L2GMap],
+                 row_map: Optional[L2GMap], nrows=None, ncols=None):
+        P = comm.size
+        if len(blocks) != P:
+            raise SpmvError(_lib.ERROR_INVALID_ARGUMENT,
+                            "spmv::Matrix - Error: need one block per rank")
+        self.comm, self._col_map, self._row_map = comm, col_map, row_map
+        rps, cis, vas = [], [], []
+        for (rp, ci, va) in blocks:
+            rps.append(np.ascontiguousarray(rp, dtype=np.int32))
+            cis.append(np.ascontiguousarray(ci, dtype=np.int32))
+            vas.append(np.ascontiguousarray(va))
+        dts = {v.dtype for v in vas}
+        if len(dts) != 1 or next(iter(dts)) not in _DTYPES:
+            raise SpmvError(_lib.ERROR_INVALID_ARGUMENT,
+                            "spmv::Matrix - Error: values need one supported dtype")
+        self.np_dtype = next(iter(dts))
+        self.dtype = _DTYPES[self.np_dtype]
+        if nrows is None:
+            nrows = [len(rp) - 1 for rp in rps]
+        if ncols is None:
+            if col_map is None:
+                raise SpmvError(_lib.ERROR_INVALID_ARGUMENT,
+                                "spmv::Matrix - Error: ncols needed without col_map")
+            ncols = [col_map.vec_len(r) for r in range(P)]
+        nr = (C.c_int32 * P)(*nrows)
+        nc = (C.c_int32 * P)(*ncols)
+        h = C.c_void_p()
+        call("spmv_matrix_create_csr", comm.handle, self.dtype,
+             col_map.handle if col_map else None, row_map.handle if row_map else None,
+             nr, nc, ptr_array([a.ctypes.data for a in rps]),
+             ptr_array([a.ctypes.data for a in cis]),
+             ptr_array([a.ctypes.data for a in vas]), C.byref(h))
+        self._h = h
+        self.nrows = list(nrows)
+        self.ncols = list(ncols)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def row_map(self) -> Optional[L2GMap]:
+        return self._row_map
+
+    def col_map(self) -> Optional[L2GMap]:
+        return self._col_map
+
+    def nnz(self, rank: int) -> int:
+        v = C.c_int64()
+        call("spmv_matrix_nnz", self._h, rank, C.byref(v))
+        return v.value
+
+    def mat(self, rank: int):
+        """Matrix::mat(): copies of rank's host CSR arrays."""
+        rp, ci, va = C.POINTER(C.c_int32)(), C.POINTER(C.c_int32)(), C.c_void_p()
+        call("spmv_matrix_csr", self._h, rank, C.byref(rp), C.byref(ci), C.byref(va))
+        m, nnz = self.nrows[rank], self.nnz(rank)
+        rpa = np.ctypeslib.as_array(rp, (m + 1,)).copy()
+        cia = np.ctypeslib.as_array(ci, (nnz,)).copy() if nnz else np.zeros(0, np.int32)
+        buf = (C.c_char * (nnz * self.np_dtype.itemsize)).from_address(va.value) \
+            if nnz else b""
+        vaa = np.frombuffer(bytes(buf), dtype=self.np_dtype).copy()
+        return rpa, cia, vaa
+
+    def set_values(self, values: Sequence) -> None:
+        mem, dt, ptrs = _vec_info(values)
+        call("spmv_matrix_set_values", self._h, mem, ptr_array(ptrs))
+
+    def set_kernel(self, kernel: str = "auto", width: int = 0, block: int = 0) -> None:
+        k = {"auto": _lib.KERNEL_AUTO, "vector": _lib.KERNEL_VECTOR,
+             "merge": _lib.KERNEL_MERGE}[kernel]
+        call("spmv_matrix_set_kernel", self._h, k, width, block)
+
+    def get_kernel(self):
+        k, w, b = C.c_int(), C.c_int(), C.c_int()
+        call("spmv_matrix_get_kernel", self._h, C.byref(k), C.byref(w), C.byref(b))
+        return {0: "auto", 1: "vector", 2: "merge"}[k.value], w.value, b.value
+
+    def _alloc_like(self, x0, lens):
+        if _is_torch(x0):
+            import torch
+            return [torch.empty(n, dtype=x0.dtype, device=x0.device) for n in lens]
+        return [np.empty(n, dtype=x0.dtype) for n in lens]
+
+    def mult(self, x: Sequence, out: Optional[List] = None) -> List:
+        """Matrix::operator* (Matrix.cpp:158-166): y[r] = A[r] x[r]."""
+        mem, dt, ptrs = _vec_info(x)
+        y = out if out is not None else self._alloc_like(x[0], self.nrows)
+        _, _, yptrs = _vec_info(y)
+        call("spmv_matrix_mult", self._h, mem, ptr_array(ptrs), ptr_array(yptrs))
+        return y
+
+    __mul__ = mult
+
+    def transpmult(self, x: Sequence, out: Optional[List] = None) -> List:
+        """Matrix::transpmult (Matrix.cpp:168-176): y[r] = A[r]^T x[r]."""
+        mem, dt, ptrs = _vec_info(x)
+        y = out if out is not None else self._alloc_like(x[0], self.ncols)
+        _, _, yptrs = _vec_info(y)
+        call("spmv_matrix_transpmult", self._h, mem, ptr_array(ptrs), ptr_array(yptrs))
+        return y
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.lib().spmv_matrix_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cg(comm: Comm, A: Matrix, b: Sequence, max_its: int, rtol: float,
+       x: Optional[List] = None, info: bool = False):
+    """spmv::cg (cg.cpp:11-83) on all ranks: returns (x, k), x[r] of length
+    col_map local_size + num_ghosts (ghost tail zero).  With info=True returns
+    (x, k, CgInfo)."""
+    if comm is not A.comm:
+        raise SpmvError(_lib.ERROR_INVALID_ARGUMENT, "spmv::cg - Error: comm mismatch")
+    mem, dt, bptrs = _vec_info(b)
+    cm = A.col_map()
+    if x is None:
+        lens = [cm.vec_len(r) for r in range(comm.size)] if cm else A.ncols
+        x = A._alloc_like(b[0], lens)
+    _, _, xptrs = _vec_info(x)
+    rows = (C.c_int64 * comm.size)(*[len(v) for v in b])
+    ci = _lib.CgInfo()
+    st = _lib.lib().spmv_cg_ex(A.handle, mem, ptr_array(bptrs), rows, ptr_array(xptrs),
+                               int(max_its), float(rtol), C.byref(ci))
+    _lib.check(st)
+    if info:
+        return x, ci.iterations, ci
+    return x, ci.iterations

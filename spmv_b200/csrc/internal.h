@@ -1,0 +1,265 @@
+// Internal declarations of libspmv_b200: handle structs, error plumbing and
+// the kernel-launch interfaces shared between the translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "spmv_b200.h"
+
+namespace spmvb {
+
+// ---------------------------------------------------------------------------
+// Errors.  Every entry point converts an spmvb::Error (or std::exception) into
+// a status code and stores the message for spmv_last_error().
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+  int status;
+  Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] inline void fail(int status, const std::string& msg) {
+  throw Error(status, msg);
+}
+inline void require(bool ok, const std::string& msg) {
+  if (!ok) fail(SPMV_ERROR_INVALID_ARGUMENT, msg);
+}
+
+void set_last_error(const std::string& msg);
+
+#define SPMVB_CUDA(call)                                                     \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess)                                                   \
+      ::spmvb::fail(e_ == cudaErrorMemoryAllocation ? SPMV_ERROR_OUT_OF_MEMORY \
+                                                    : SPMV_ERROR_CUDA,       \
+                    std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+// Runs `body` and turns exceptions into a status code.
+template <class F>
+int guard(F&& body) {
+  try {
+    body();
+    return SPMV_SUCCESS;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    set_last_error("spmv: host allocation failed");
+    return SPMV_ERROR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return SPMV_ERROR_INTERNAL;
+  }
+}
+
+inline size_t dtype_size(spmv_dtype t) {
+  switch (t) {
+    case SPMV_FLOAT64: return 8;
+    case SPMV_FLOAT32: return 4;
+    case SPMV_COMPLEX64: return 8;
+    case SPMV_COMPLEX128: return 16;
+  }
+  fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: unknown dtype");
+}
+
+// ---------------------------------------------------------------------------
+// Device buffer (RAII, cudaMalloc/cudaFree on the owning device).
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes) {
+    o.ptr = nullptr;
+    o.bytes = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      ptr = o.ptr;
+      bytes = o.bytes;
+      o.ptr = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  // Grows (never shrinks) to at least `n` bytes; contents are not kept.
+  void reserve(size_t n) {
+    if (n <= bytes) return;
+    release();
+    if (n == 0) return;
+    SPMVB_CUDA(cudaMalloc(&ptr, n));
+    bytes = n;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Selects the communicator's device for the lifetime of the guard.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev);
+  ~DeviceGuard();
+};
+
+}  // namespace spmvb
+
+// ---------------------------------------------------------------------------
+// Handles
+// ---------------------------------------------------------------------------
+struct spmv_comm_s {
+  int device = -1;          // -1: host-only
+  int size = 0;             // number of virtual ranks
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int num_sms = 0;
+  // Staging buffers for SPMV_MEMORY_HOST calls.
+  spmvb::DevBuf stage_in, stage_out;
+  void require_device() const {
+    if (device < 0)
+      spmvb::fail(SPMV_ERROR_NO_DEVICE,
+                  "spmv: communicator has no CUDA device");
+  }
+};
+
+namespace spmvb {
+
+// Communication pattern of one rank, as L2GMap.cpp:15-122 computes it.
+struct RankMap {
+  int64_t local_size = 0;
+  std::vector<int64_t> ghosts;
+  std::vector<int32_t> neighbours, send_count, recv_count, send_offset,
+      recv_offset, indexbuf;
+};
+
+// Device tables derived from the pattern.
+struct HaloTables {
+  bool built = false;
+  int64_t n_update = 0;   // ghost slots over all ranks
+  int64_t n_targets = 0;  // distinct (rank, owned index) reverse targets
+  int64_t n_contrib = 0;  // reverse contributions
+  DevBuf upd_ranks;       // int32: (dst_rank << 16) | src_rank
+  DevBuf upd_dst;         // int32 dst index in dst rank's vector
+  DevBuf upd_src;         // int32 src index in src rank's vector
+  DevBuf rev_tgt_rank;    // int32
+  DevBuf rev_tgt_idx;     // int32
+  DevBuf rev_ptr;         // int32 [n_targets+1]
+  DevBuf rev_src_rank;    // int32 [n_contrib]
+  DevBuf rev_src_idx;     // int32 [n_contrib]
+};
+
+}  // namespace spmvb
+
+struct spmv_l2gmap_s {
+  spmv_comm comm = nullptr;
+  std::vector<int64_t> ranges;           // [size+1]
+  std::vector<spmvb::RankMap> rank;      // [size]
+  spmvb::HaloTables halo;
+  int64_t vec_len(int r) const {
+    return rank[r].local_size + (int64_t)rank[r].ghosts.size();
+  }
+};
+
+namespace spmvb {
+
+// One rank's block of a concatenated CSR on the device.
+struct DevPart {
+  int32_t nrows = 0, ncols = 0;
+  int64_t nnz = 0;
+  int64_t rp_off = 0;   // offset of this rank's rowptr in the concatenation
+  int64_t nz_off = 0;   // offset of this rank's entries (aligned to 4)
+};
+
+// A device CSR (all ranks concatenated) plus the derived column arrays.
+struct DevCsr {
+  std::vector<DevPart> parts;
+  int64_t rp_total = 0, nz_total = 0;   // allocated lengths (with padding)
+  DevBuf rowptr;        // int32
+  DevBuf cols;          // int32: rank-local column indices
+  DevBuf vals;          // scalar of the matrix dtype
+  DevBuf cols_global;   // int32: global column indices (fused-halo layout)
+  DevBuf vals32;        // float copy of FP64 values (mixed precision)
+  // Row statistics (over all ranks).
+  double mean_row = 0;
+  int64_t max_row = 0;
+};
+
+}  // namespace spmvb
+
+struct CgWorkspace;  // cg.cu
+
+struct spmv_matrix_s {
+  spmv_comm comm = nullptr;
+  spmv_dtype dtype = SPMV_FLOAT64;
+  spmv_l2gmap col_map = nullptr, row_map = nullptr;
+  // Host copies (Matrix::mat()).
+  std::vector<std::vector<int32_t>> h_rowptr, h_colind;
+  std::vector<std::vector<unsigned char>> h_vals;
+  std::vector<int32_t> nrows, ncols;
+  // Device plans.
+  spmvb::DevCsr fwd;            // A
+  spmvb::DevCsr trn;            // A^T, built on first transpmult
+  bool trn_built = false;
+  // Kernel choice.
+  spmv_kernel kernel = SPMV_KERNEL_AUTO;
+  int width = 0, block = 0;
+  std::unique_ptr<CgWorkspace, void (*)(CgWorkspace*)> cg{nullptr, nullptr};
+};
+
+namespace spmvb {
+
+// ---------------------------------------------------------------------------
+// Kernel-launch interfaces (implemented in the .cu files)
+// ---------------------------------------------------------------------------
+struct SpmvLaunch {
+  const DevCsr* csr;
+  const int32_t* cols;                 // csr->cols or csr->cols_global
+  spmv_dtype dtype;
+  const void* const* x;                // [nparts] device pointers
+  void* const* y;                      // [nparts]
+  spmv_kernel kernel;
+  int width, block;
+  int num_sms;
+};
+void launch_spmv(const SpmvLaunch& L, cudaStream_t stream);
+// Lanes per row picked from the mean row length (vector kernel).
+int auto_width(double mean_row, spmv_dtype dtype);
+int max_blocks_for(int num_sms, int BS);
+
+void build_halo_tables(spmv_l2gmap map);
+void launch_update(spmv_l2gmap map, spmv_dtype dtype, void* const* vecs,
+                   cudaStream_t stream);
+void launch_reverse_update(spmv_l2gmap map, spmv_dtype dtype,
+                           void* const* vecs, cudaStream_t stream);
+
+// Build the L2GMap pattern on the host (all ranks).
+void build_pattern(spmv_l2gmap map, const int64_t* local_size,
+                   const int64_t* const* ghosts, const int64_t* num_ghosts);
+
+void upload_csr(spmv_matrix A);
+void build_transpose(spmv_matrix A);
+void build_global_cols(spmv_matrix A);
+
+// CG in the fused-halo (global) layout: cg_rhs/cg_solution are the device
+// vectors of length global_size that cg_run reads b from and leaves x in.
+double* cg_rhs(spmv_matrix A);
+double* cg_solution(spmv_matrix A);
+void cg_run(spmv_matrix A, int max_its, double rtol, spmv_cg_info* info);
+void destroy_cg_workspace(CgWorkspace* w);
+
+}  // namespace spmvb

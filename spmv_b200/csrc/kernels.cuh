@@ -1,0 +1,139 @@
+// Device-side building blocks shared by the kernels: kernel-parameter tables,
+// vector types, cache-hinted loads and deterministic block reductions.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "spmv_b200.h"
+
+namespace spmvb {
+
+// Per-rank descriptor of one launch over a concatenated CSR.  A launch covers
+// all ranks; rank p owns CTAs [block_begin, block_begin + nblocks), which
+// stride over its ntiles row tiles.
+struct PartArg {
+  const int32_t* rowptr;   // rank's row pointers (nrows+1), relative to vals
+  const int32_t* cols;     // rank's column indices
+  const void* vals;        // rank's values
+  const void* x;           // input vector the column indices refer to
+  void* y;                 // output rows
+  const void* xown;        // this rank's own entries of x (row-aligned)
+  int32_t nrows;
+  int32_t block_begin;
+  int32_t nblocks;
+  int32_t ntiles;
+};
+
+struct SpmvArgs {
+  int32_t nparts;
+  int32_t nblocks;
+  PartArg part[SPMV_MAX_PARTS];
+};
+
+// Pointer per rank, for the halo kernels.
+struct PtrTable {
+  void* p[SPMV_MAX_PARTS];
+};
+
+template <typename T>
+struct VecT;
+template <>
+struct VecT<double> {
+  static constexpr int N = 2;  // 16-byte value loads
+  using V = double2;
+  using C = int2;
+};
+template <>
+struct VecT<float> {
+  static constexpr int N = 4;
+  using V = float4;
+  using C = int4;
+};
+
+__device__ __forceinline__ double comp(const double2& v, int i) {
+  return i == 0 ? v.x : v.y;
+}
+__device__ __forceinline__ float comp(const float4& v, int i) {
+  return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ int comp(const int2& v, int i) {
+  return i == 0 ? v.x : v.y;
+}
+__device__ __forceinline__ int comp(const int4& v, int i) {
+  return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+}
+
+// Streaming loads for matrix data (read once per product): evict-first.
+template <typename V>
+__device__ __forceinline__ V ld_stream(const V* p) {
+  return __ldcs(p);
+}
+// Read-only cached load for gathered vector entries.
+template <typename T>
+__device__ __forceinline__ T ld_gather(const T* p) {
+  return __ldg(p);
+}
+
+// Rank owning CTA `b` of a launch (ranks' CTA ranges are ascending).
+__device__ __forceinline__ int find_part(const SpmvArgs& a, int b) {
+  int lo = 0, hi = a.nparts - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (a.part[mid].block_begin <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Sum over the CTA; the result is valid in thread 0.  The order of additions
+// depends only on blockDim, so results are reproducible run to run.
+template <int BS>
+__device__ __forceinline__ double block_sum(double v, double* smem) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) smem[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = lane < (BS >> 5) ? smem[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  __syncthreads();
+  return v;
+}
+
+// Single-pass grid reduction: every CTA stores its partial; the last CTA to
+// arrive (atomic ticket) sums all partials in index order and returns true in
+// all of its threads with the total in *total (valid in thread 0).  The
+// ticket counter is reset by the last CTA so the kernel can be relaunched.
+// No CTA waits for another: there is no spin loop.
+template <int BS>
+__device__ __forceinline__ bool grid_sum(double part, double* partials,
+                                         unsigned int* ticket, double* total,
+                                         double* smem) {
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = part;
+    __threadfence();
+    const unsigned int t = atomicAdd(ticket, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  double v = 0.0;
+  for (unsigned int i = threadIdx.x; i < gridDim.x; i += BS)
+    v += __ldcg(partials + i);
+  v = block_sum<BS>(v, smem);
+  if (threadIdx.x == 0) {
+    *total = v;
+    *ticket = 0u;
+  }
+  return true;
+}
+
+}  // namespace spmvb

@@ -1,0 +1,133 @@
+"""Matrix::operator* and transpmult on the GPU against the oracle's
+restatement of the reference's Eigen products (Matrix.cpp:199-211)."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import spmv_b200 as S
+from spmv_b200 import gen
+from helpers import (TOL_F32, TOL_F64, abs_mult, assert_spmv_close, build,
+                     random_csr)
+
+pytestmark = pytest.mark.gpu
+
+
+def check_mult(M, D, xs, tol, device=False):
+    if device:
+        xt = [torch.from_numpy(x).cuda() for x in xs]
+        ys = [y.cpu().numpy() for y in M.mult(xt)]
+    else:
+        ys = M.mult(xs)
+    for q in range(D.P):
+        rp, ci, va = D.blocks[q]
+        yref = oracle.csr_mult(rp, ci, va, xs[q])
+        assert_spmv_close(ys[q], yref, abs_mult(D.blocks[q], xs[q]), tol)
+    return ys
+
+
+@pytest.mark.parametrize("cfg,P", [("c1", 1), ("c2", 8), ("c2", 3), ("c1", 2)])
+def test_mult_matches_oracle(cuda_device, cfg, P):
+    W = gen.workload(cfg)
+    comm, cm, rm, M, D = build(W, P)
+    rng = np.random.default_rng(0)
+    xs = [rng.uniform(-1, 1, cm.vec_len(q)) for q in range(P)]
+    y_host = check_mult(M, D, xs, TOL_F64)
+    y_dev = check_mult(M, D, xs, TOL_F64, device=True)
+    for a, b in zip(y_host, y_dev):
+        assert np.array_equal(a, b)  # same kernel, same order: bitwise
+
+
+def test_mult_float32(cuda_device):
+    W = gen.workload("c2", scale=48)
+    comm, cm, rm, M, D = build(W, 4, dtype=np.float32)
+    rng = np.random.default_rng(1)
+    xs = [rng.uniform(-1, 1, cm.vec_len(q)).astype(np.float32) for q in range(4)]
+    check_mult(M, D, xs, TOL_F32)
+    check_mult(M, D, xs, TOL_F32, device=True)
+
+
+@pytest.mark.parametrize("width", [1, 2, 4, 8, 16, 32])
+@pytest.mark.parametrize("block", [128, 256, 512])
+def test_every_width_and_block(cuda_device, width, block):
+    rng = np.random.default_rng(width * 1000 + block)
+    A = random_csr(rng, 3001, 3001, density=0.004, long_rows=(7, 2500))
+    comm, cm, rm, M, D = build(A, 3)
+    M.set_kernel("vector", width, block)
+    assert M.get_kernel() == ("vector", width, block)
+    xs = [rng.standard_normal(cm.vec_len(q)) for q in range(3)]
+    check_mult(M, D, xs, TOL_F64)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_ragged_random_matrices(cuda_device, seed):
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(1, 4000))
+    P = int(rng.integers(1, 9))
+    A = random_csr(rng, n, n, density=float(rng.uniform(0.0, 0.02)),
+                   long_rows=tuple(rng.integers(0, n, size=2)),
+                   empty_frac=float(rng.uniform(0, 0.5)))
+    comm, cm, rm, M, D = build(A, min(P, n))
+    xs = [rng.standard_normal(cm.vec_len(q)) for q in range(D.P)]
+    check_mult(M, D, xs, TOL_F64)
+    M32 = S.Matrix(comm, [(rp, ci, va.astype(np.float32)) for rp, ci, va in D.blocks],
+                   cm, rm)
+    ys = M32.mult([x.astype(np.float32) for x in xs])
+    for q in range(D.P):
+        rp, ci, va = D.blocks[q]
+        yref = oracle.csr_mult(rp, ci, va.astype(np.float32), xs[q].astype(np.float32))
+        assert_spmv_close(ys[q], yref, abs_mult(D.blocks[q], xs[q]).astype(np.float32),
+                          TOL_F32)
+
+
+def test_empty_and_zero_row_ranks(cuda_device):
+    # A rank with no rows, a matrix with no entries, a 1x1 matrix.
+    comm = S.Comm(size=3, device=0)
+    cm = S.L2GMap(comm, [0, 2, 1], [[], [], []])
+    blocks = [(np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0)),
+              (np.array([0, 0, 0], np.int32), np.zeros(0, np.int32), np.zeros(0)),
+              (np.array([0, 1], np.int32), np.array([0], np.int32), np.array([2.5]))]
+    M = S.Matrix(comm, blocks, cm, cm)
+    ys = M.mult([np.zeros(0), np.ones(2), np.array([3.0])])
+    assert ys[0].size == 0 and np.array_equal(ys[1], [0, 0]) and ys[2][0] == 7.5
+
+
+@pytest.mark.parametrize("cfg,P", [("c2", 8), ("c1", 1)])
+def test_transpmult_matches_oracle(cuda_device, cfg, P):
+    W = gen.workload(cfg, scale=40 if cfg == "c2" else 0)
+    comm, cm, rm, M, D = build(W, P)
+    rng = np.random.default_rng(2)
+    xs = [rng.uniform(-1, 1, D.local_sizes[q]) for q in range(P)]
+    ys = M.transpmult(xs)
+    for q in range(P):
+        rp, ci, va = D.blocks[q]
+        n = cm.vec_len(q)
+        yref = oracle.csr_transpmult(rp, ci, va, xs[q], n)
+        absx = oracle.csr_transpmult(rp, ci, np.abs(va), np.abs(xs[q]), n)
+        assert ys[q].shape == (n,)
+        assert_spmv_close(ys[q], yref, absx, TOL_F64)
+
+
+def test_transpmult_ragged(cuda_device):
+    rng = np.random.default_rng(9)
+    A = random_csr(rng, 1500, 1500, density=0.01, long_rows=(3,))
+    comm, cm, rm, M, D = build(A, 4)
+    xs = [rng.standard_normal(D.local_sizes[q]) for q in range(4)]
+    ys = M.transpmult(xs)
+    for q in range(4):
+        rp, ci, va = D.blocks[q]
+        n = cm.vec_len(q)
+        assert_spmv_close(ys[q], oracle.csr_transpmult(rp, ci, va, xs[q], n),
+                          oracle.csr_transpmult(rp, ci, np.abs(va), np.abs(xs[q]), n),
+                          TOL_F64)
+
+
+def test_set_values_keeps_pattern(cuda_device):
+    W = gen.workload("c1", scale=64)
+    comm, cm, rm, M, D = build(W, 2)
+    new = [va * 2.0 for (_, _, va) in D.blocks]
+    M.set_values(new)
+    D.blocks = [(rp, ci, v) for (rp, ci, _), v in zip(D.blocks, new)]
+    rng = np.random.default_rng(3)
+    xs = [rng.uniform(-1, 1, cm.vec_len(q)) for q in range(2)]
+    check_mult(M, D, xs, TOL_F64)
