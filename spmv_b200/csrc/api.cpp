@@ -1,5 +1,7 @@
 // extern "C" entry points of libspmv_b200 (declared in include/spmv_b200.h).
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
@@ -13,15 +15,33 @@ thread_local std::string g_last_error;
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
+void debug_log(const std::string& msg) {
+  static const bool on = std::getenv("SPMV_B200_DEBUG") != nullptr;
+  if (on) std::fprintf(stderr, "[spmv_b200] %s\n", msg.c_str());
+}
+
+void soft_check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  (void)cudaGetLastError();
+  debug_log(std::string(what) + " failed: " + cudaGetErrorString(e));
+}
+
+// Entering device work: an error left pending by an earlier call (of this
+// library's runtime, in this thread) is cleared and logged here, so that the
+// launch checks below only ever report errors of this call.
 DeviceGuard::DeviceGuard(int dev) {
   if (dev < 0) return;
+  const cudaError_t pending = cudaGetLastError();
+  if (pending != cudaSuccess)
+    debug_log(std::string("cleared a pending error: ") + cudaGetErrorString(pending));
   SPMVB_CUDA(cudaGetDevice(&prev));
   if (prev != dev) SPMVB_CUDA(cudaSetDevice(dev));
 }
 DeviceGuard::~DeviceGuard() {
   int cur = -1;
-  if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev)
-    cudaSetDevice(prev);
+  if (prev < 0) return;
+  soft_check(cudaGetDevice(&cur), "cudaGetDevice");
+  if (cur >= 0 && cur != prev) soft_check(cudaSetDevice(prev), "cudaSetDevice");
 }
 
 namespace {
@@ -189,6 +209,28 @@ void build_transpose(spmv_matrix A) {
   A->trn_built = true;
 }
 
+void release_comm(spmv_comm comm) {
+  if (--comm->refs > 0) return;
+  if (comm->device >= 0) {
+    DeviceGuard dg(comm->device);
+    if (comm->own_stream)
+      soft_check(cudaStreamDestroy(comm->stream), "cudaStreamDestroy");
+    comm->stage_in.release();
+    comm->stage_out.release();
+  }
+  delete comm;
+}
+
+void release_map(spmv_l2gmap map) {
+  if (--map->refs > 0) return;
+  spmv_comm comm = map->comm;
+  {
+    DeviceGuard dg(comm->device);
+    delete map;
+  }
+  release_comm(comm);
+}
+
 namespace {
 
 // y = op(A) x for all ranks, host or device vectors.
@@ -218,6 +260,7 @@ void product(spmv_matrix A, bool transpose, spmv_memory memory,
   L.width = transpose ? 0 : A->width;
   L.block = A->block;
   L.num_sms = comm->num_sms;
+  L.carry = transpose ? &A->trn.merge_carry : &A->fwd.merge_carry;
   cudaStream_t s = comm->stream;
   if (memory == SPMV_MEMORY_DEVICE) {
     L.x = x;
@@ -338,14 +381,7 @@ int spmv_comm_create(int device, void* stream, int size, spmv_comm* out) {
 
 int spmv_comm_destroy(spmv_comm comm) {
   return guard([&] {
-    if (!comm) return;
-    if (comm->device >= 0) {
-      DeviceGuard dg(comm->device);
-      if (comm->own_stream) cudaStreamDestroy(comm->stream);
-      comm->stage_in.release();
-      comm->stage_out.release();
-    }
-    delete comm;
+    if (comm) release_comm(comm);
   });
 }
 
@@ -393,19 +429,14 @@ int spmv_l2gmap_create(spmv_comm comm, const int64_t* local_size,
     std::unique_ptr<spmv_l2gmap_s> m(new spmv_l2gmap_s);
     m->comm = comm;
     build_pattern(m.get(), local_size, ghosts, num_ghosts);
+    ++comm->refs;
     *out = m.release();
   });
 }
 
 int spmv_l2gmap_destroy(spmv_l2gmap map) {
   return guard([&] {
-    if (!map) return;
-    if (map->comm && map->comm->device >= 0) {
-      DeviceGuard dg(map->comm->device);
-      delete map;
-    } else {
-      delete map;
-    }
+    if (map) release_map(map);
   });
 }
 
@@ -563,6 +594,9 @@ int spmv_matrix_create_csr(spmv_comm comm, spmv_dtype dtype,
       A->h_vals[r].assign(vb, vb + nnz * es);
     }
     upload_csr(A.get());
+    ++comm->refs;
+    if (col_map) ++col_map->refs;
+    if (row_map) ++row_map->refs;
     *out = A.release();
   });
 }
@@ -570,12 +604,15 @@ int spmv_matrix_create_csr(spmv_comm comm, spmv_dtype dtype,
 int spmv_matrix_destroy(spmv_matrix A) {
   return guard([&] {
     if (!A) return;
-    if (A->comm && A->comm->device >= 0) {
-      DeviceGuard dg(A->comm->device);
-      delete A;
-    } else {
+    spmv_comm comm = A->comm;
+    spmv_l2gmap cm = A->col_map, rm = A->row_map;
+    {
+      DeviceGuard dg(comm->device);
       delete A;
     }
+    if (cm) release_map(cm);
+    if (rm) release_map(rm);
+    release_comm(comm);
   });
 }
 
@@ -706,7 +743,7 @@ int spmv_matrix_get_kernel(spmv_matrix A, spmv_kernel* kernel, int* width,
   return guard([&] {
     check_mat(A);
     require(kernel && width && block, "spmv: NULL output");
-    *kernel = A->kernel == SPMV_KERNEL_AUTO ? SPMV_KERNEL_VECTOR : A->kernel;
+    *kernel = pick_kernel(A->kernel, A->fwd);
     *width = A->width > 0 ? A->width : auto_width(A->fwd.mean_row, A->dtype);
     *block = A->block > 0 ? A->block : 256;
   });

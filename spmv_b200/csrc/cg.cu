@@ -42,8 +42,8 @@ struct CgWorkspace {
   cudaGraphConditionalHandle handle = 0;
   CgState host{};
   ~CgWorkspace() {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
+    if (exec) spmvb::soft_check(cudaGraphExecDestroy(exec), "cudaGraphExecDestroy");
+    if (graph) spmvb::soft_check(cudaGraphDestroy(graph), "cudaGraphDestroy");
   }
 };
 

@@ -31,6 +31,12 @@ inline void require(bool ok, const std::string& msg) {
 }
 
 void set_last_error(const std::string& msg);
+// Debug log (stderr) when SPMV_B200_DEBUG is set in the environment.
+void debug_log(const std::string& msg);
+// For calls whose failure must not abort the caller (frees, destroys): a
+// failure is logged and the runtime's pending error is cleared, so it cannot
+// be reported later by an unrelated call.
+void soft_check(cudaError_t e, const char* what);
 
 #define SPMVB_CUDA(call)                                                     \
   do {                                                                       \
@@ -94,7 +100,7 @@ struct DevBuf {
   }
   ~DevBuf() { release(); }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) soft_check(cudaFree(ptr), "cudaFree");
     ptr = nullptr;
     bytes = 0;
   }
@@ -128,6 +134,10 @@ struct spmv_comm_s {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int num_sms = 0;
+  // References: the caller's handle plus one per live map or matrix, so the
+  // communicator outlives everything created on it, whatever the order of
+  // the destroy calls.
+  int refs = 1;
   // Staging buffers for SPMV_MEMORY_HOST calls.
   spmvb::DevBuf stage_in, stage_out;
   void require_device() const {
@@ -167,6 +177,7 @@ struct HaloTables {
 
 struct spmv_l2gmap_s {
   spmv_comm comm = nullptr;
+  int refs = 1;  // caller's handle plus one per matrix using the map
   std::vector<int64_t> ranges;           // [size+1]
   std::vector<spmvb::RankMap> rank;      // [size]
   spmvb::HaloTables halo;
@@ -194,6 +205,7 @@ struct DevCsr {
   DevBuf vals;          // scalar of the matrix dtype
   DevBuf cols_global;   // int32: global column indices (fused-halo layout)
   DevBuf vals32;        // float copy of FP64 values (mixed precision)
+  DevBuf merge_carry;   // per-CTA carries of the merge-path product
   // Row statistics (over all ranks).
   double mean_row = 0;
   int64_t max_row = 0;
@@ -235,8 +247,13 @@ struct SpmvLaunch {
   spmv_kernel kernel;
   int width, block;
   int num_sms;
+  DevBuf* carry;                       // merge-path scratch (per matrix)
 };
 void launch_spmv(const SpmvLaunch& L, cudaStream_t stream);
+void launch_merge(const SpmvLaunch& L, cudaStream_t stream, DevBuf& carry);
+// Kernel family for a matrix: the caller's choice, or from row statistics
+// (merge-path when the longest row is far above the mean).
+spmv_kernel pick_kernel(spmv_kernel requested, const DevCsr& C);
 // Lanes per row picked from the mean row length (vector kernel).
 int auto_width(double mean_row, spmv_dtype dtype);
 int max_blocks_for(int num_sms, int BS);
@@ -250,6 +267,10 @@ void launch_reverse_update(spmv_l2gmap map, spmv_dtype dtype,
 // Build the L2GMap pattern on the host (all ranks).
 void build_pattern(spmv_l2gmap map, const int64_t* local_size,
                    const int64_t* const* ghosts, const int64_t* num_ghosts);
+
+// Drop one reference, freeing the object with the last one.
+void release_comm(spmv_comm comm);
+void release_map(spmv_l2gmap map);
 
 void upload_csr(spmv_matrix A);
 void build_transpose(spmv_matrix A);

@@ -89,6 +89,12 @@ void launch_vector_bs(const SpmvArgs& a, int W, int BS, cudaStream_t s) {
 
 }  // namespace
 
+spmv_kernel pick_kernel(spmv_kernel requested, const DevCsr& C) {
+  if (requested != SPMV_KERNEL_AUTO) return requested;
+  const double skew_limit = std::max(64.0, 8.0 * C.mean_row);
+  return double(C.max_row) > skew_limit ? SPMV_KERNEL_MERGE : SPMV_KERNEL_VECTOR;
+}
+
 int max_blocks_for(int num_sms, int BS) {
   // One wave of resident CTAs (2048 threads per SM), times two so that a
   // CTA finishing early finds work without waiting for the tail.
@@ -104,8 +110,11 @@ void launch_spmv(const SpmvLaunch& L, cudaStream_t stream) {
           "spmv: width must be 1..32, a power of two");
   require(BS == 128 || BS == 256 || BS == 512,
           "spmv: block must be 128, 256 or 512");
-  require(L.kernel == SPMV_KERNEL_AUTO || L.kernel == SPMV_KERNEL_VECTOR,
-          "spmv: the merge-path kernel is not available in this build");
+  if (pick_kernel(L.kernel, *L.csr) == SPMV_KERNEL_MERGE) {
+    require(L.carry != nullptr, "spmv: merge-path product needs a carry buffer");
+    launch_merge(L, stream, *L.carry);
+    return;
+  }
   SpmvArgs a;
   const size_t es = dtype_size(L.dtype);
   fill_spmv_args(a, *L.csr, L.cols, es, L.x, L.y, nullptr, BS / W,

@@ -67,3 +67,35 @@ def test_matrix_validation_messages():
     assert np.array_equal(rpa, rp) and np.array_equal(cia, [0, 1, 2])
     assert np.array_equal(vaa, np.ones(3))
     assert A.get_kernel() == ("vector", 1, 256) or A.get_kernel()[0] == "vector"
+
+
+def test_destroy_order_does_not_matter():
+    # The communicator and maps are reference counted by what uses them, as
+    # the reference's Matrix holds its maps by shared_ptr.
+    L = _lib.lib()
+    comm = C.c_void_p()
+    _lib.call("spmv_comm_create", -1, None, 1, C.byref(comm))
+    ls = (C.c_int64 * 1)(3)
+    g = (C.POINTER(C.c_int64) * 1)()
+    ng = (C.c_int64 * 1)(0)
+    cm = C.c_void_p()
+    _lib.call("spmv_l2gmap_create", comm, ls, g, ng, C.byref(cm))
+    rp = np.array([0, 1, 2, 3], np.int32)
+    ci = np.array([0, 1, 2], np.int32)
+    va = np.ones(3)
+    A = C.c_void_p()
+    _lib.call("spmv_matrix_create_csr", comm, _lib.FLOAT64, cm, cm, (C.c_int32 * 1)(3),
+              (C.c_int32 * 1)(3), _lib.ptr_array([rp.ctypes.data]),
+              _lib.ptr_array([ci.ctypes.data]), _lib.ptr_array([va.ctypes.data]),
+              C.byref(A))
+    assert L.spmv_comm_destroy(comm) == 0
+    assert L.spmv_l2gmap_destroy(cm) == 0
+    n = C.c_int64()
+    _lib.call("spmv_matrix_nnz", A, 0, C.byref(n))  # still usable
+    assert n.value == 3
+    m = C.c_void_p()
+    _lib.call("spmv_matrix_col_map", A, C.byref(m))
+    gs = C.c_int64()
+    _lib.call("spmv_l2gmap_global_size", m, C.byref(gs))
+    assert gs.value == 3
+    assert L.spmv_matrix_destroy(A) == 0

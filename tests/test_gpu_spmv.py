@@ -131,3 +131,48 @@ def test_set_values_keeps_pattern(cuda_device):
     rng = np.random.default_rng(3)
     xs = [rng.uniform(-1, 1, cm.vec_len(q)) for q in range(2)]
     check_mult(M, D, xs, TOL_F64)
+
+
+@pytest.mark.parametrize("seed", range(5))
+def test_merge_path_matches_oracle(cuda_device, seed):
+    rng = np.random.default_rng(500 + seed)
+    n = int(rng.integers(50, 5000))
+    A = random_csr(rng, n, n, density=float(rng.uniform(0.0, 0.01)),
+                   long_rows=tuple(rng.integers(0, n, size=3)),
+                   empty_frac=float(rng.uniform(0, 0.6)))
+    P = int(rng.integers(1, 5))
+    comm, cm, rm, M, D = build(A, P)
+    M.set_kernel("merge")
+    assert M.get_kernel()[0] == "merge"
+    xs = [rng.standard_normal(cm.vec_len(q)) for q in range(P)]
+    ys1 = check_mult(M, D, xs, TOL_F64)
+    ys2 = M.mult(xs)
+    assert all(np.array_equal(a, b) for a, b in zip(ys1, ys2))  # reproducible
+    xt = [rng.standard_normal(D.local_sizes[q]) for q in range(P)]
+    yt = M.transpmult(xt)
+    for q in range(P):
+        rp, ci, va = D.blocks[q]
+        nc = cm.vec_len(q)
+        assert_spmv_close(yt[q], oracle.csr_transpmult(rp, ci, va, xt[q], nc),
+                          oracle.csr_transpmult(rp, ci, np.abs(va), np.abs(xt[q]), nc),
+                          TOL_F64)
+
+
+def test_auto_picks_merge_for_a_dense_row(cuda_device):
+    n = 20000
+    rng = np.random.default_rng(7)
+    lens = np.full(n, 3)
+    lens[17] = n  # one full row
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    cols = np.concatenate([np.sort(rng.choice(n, size=k, replace=False)) for k in lens])
+    A = gen.CSR(rp, cols.astype(np.int32), rng.standard_normal(rp[-1]), n)
+    comm, cm, rm, M, D = build(A, 1)
+    assert M.get_kernel()[0] == "merge"
+    xs = [rng.standard_normal(n)]
+    check_mult(M, D, xs, TOL_F64)
+    M32 = S.Matrix(comm, [(rp, cols.astype(np.int32), D.blocks[0][2].astype(np.float32))],
+                   cm, rm)
+    y32 = M32.mult([xs[0].astype(np.float32)])[0]
+    yref = oracle.csr_mult(rp, cols.astype(np.int32), D.blocks[0][2].astype(np.float32),
+                           xs[0].astype(np.float32))
+    assert_spmv_close(y32, yref, abs_mult(D.blocks[0], xs[0]).astype(np.float32), TOL_F32)
