@@ -191,6 +191,33 @@ int spmv_matrix_row_map(spmv_matrix A, spmv_l2gmap* map);
 /* Replace the values of every rank (same sparsity pattern).  values[size]. */
 int spmv_matrix_set_values(spmv_matrix A, spmv_memory memory,
                            const void* const* values);
+/* Allocation-free product y[r] = A[r] x[r] (no counterpart in the reference).
+ *
+ * For callers that must not allocate device memory while they run: an
+ * application whose device memory is handed out by its own allocator or pool,
+ * sized at start-up, cannot have a library call cudaMalloc behind its back (the
+ * call fails when the pool already holds the memory, and cudaMalloc/cudaFree
+ * can stall the whole device in the middle of a time-critical loop).
+ * spmv_matrix_mult's merge-path kernel keeps per-CTA partial row sums in a
+ * buffer the library allocates on first use; this entry point runs the same
+ * merge-path kernels with those partial sums in a fixed device array that is
+ * part of the library (192 KiB, kept on every device that loads the library
+ * until the process exits), so a call allocates nothing.
+ *  - x and y are device pointers, one per rank, as for spmv_matrix_mult with
+ *    SPMV_MEMORY_DEVICE; the work is ordered on the communicator's stream.
+ *  - Limit: rows + nonzeros over all ranks of at most 33,554,432 (16384 tiles
+ *    of 2048); a larger matrix is rejected with SPMV_ERROR_INVALID_ARGUMENT.
+ *  - The first call on a device looks up the array's device address, once per
+ *    device; make that first call before any stream capture.
+ *  - All calls share the one array, which keeps what the last call left in it
+ *    (each call writes every slot before reading it, so nothing needs
+ *    clearing); calls that overlap on the GPU, e.g. from two streams of the
+ *    same device, race on it and must not be issued.
+ *  - Results equal spmv_matrix_mult's within rounding (FP64: 1e-12 of
+ *    (|A||x|) per row); bitwise when that matrix also uses the merge-path
+ *    kernel. */
+int spmv_matrix_mult_noalloc(spmv_matrix A, const void* const* x,
+                             void* const* y);
 /* Kernel choice.  width: lanes per row for SPMV_KERNEL_VECTOR (1..32, power
  * of two; 0 = from statistics); block: threads per CTA (0 = default). */
 int spmv_matrix_set_kernel(spmv_matrix A, spmv_kernel kernel, int width,

@@ -86,6 +86,7 @@ _SIGS = {
     "spmv_matrix_col_map": [_p, C.POINTER(_p)],
     "spmv_matrix_row_map": [_p, C.POINTER(_p)],
     "spmv_matrix_set_values": [_p, _int, _pp],
+    "spmv_matrix_mult_noalloc": [_p, _pp, _pp],
     "spmv_matrix_set_kernel": [_p, _int, _int, _int],
     "spmv_matrix_get_kernel": [_p, C.POINTER(_int), C.POINTER(_int), C.POINTER(_int)],
     "spmv_cg": [_p, _int, _pp, C.POINTER(_i64), _pp, _int, C.c_double,

@@ -16,6 +16,9 @@
 // goes to a per-CTA slot, and merge_fixup adds each run of carries that
 // belong to one row, in CTA order, to that row.
 #include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
 
 #include "internal.h"
 #include "kernels.cuh"
@@ -200,4 +203,98 @@ void launch_merge(const SpmvLaunch& L, cudaStream_t stream, DevBuf& carry) {
   SPMVB_CUDA(cudaGetLastError());
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free product: spmv_matrix_mult_noalloc.
+//
+// The merge-path product above keeps its per-CTA carries in a buffer that
+// spmv_matrix_mult allocates (and grows) on demand.  This variant runs the
+// same two kernels with the carries in a fixed file-scope device array, so a
+// call allocates no device memory.  The array holds NOALLOC_MAX_TILES tiles of
+// TILE (= 2048) merge items, i.e. rows + nonzeros of all ranks together up to
+// 16384 * 2048 = 33,554,432; it is 192 KiB and stays resident on every
+// device that loads this library until the process exits.
+// ---------------------------------------------------------------------------
+constexpr int NOALLOC_MAX_TILES = 16384;
+constexpr size_t NOALLOC_VAL_OFFSET = size_t(NOALLOC_MAX_TILES) * sizeof(int);
+static __device__ __align__(256) unsigned char
+    g_noalloc_carry[NOALLOC_VAL_OFFSET + size_t(NOALLOC_MAX_TILES) * sizeof(double)];
+
+namespace {
+
+// Device address of g_noalloc_carry, looked up once per device (with that
+// device current).  Host code must not use the symbol's name as an address:
+// on the host it names a shadow object, not device memory.
+void* noalloc_scratch(int device) {
+  static std::mutex mu;
+  static std::vector<void*> addr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (int(addr.size()) <= device) addr.resize(device + 1, nullptr);
+  if (!addr[device]) {
+    void* p = nullptr;
+    SPMVB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_carry));
+    addr[device] = p;
+  }
+  return addr[device];
+}
+
+}  // namespace
+
 }  // namespace spmvb
+
+extern "C" int spmv_matrix_mult_noalloc(spmv_matrix A, const void* const* x,
+                                        void* const* y) {
+  using namespace spmvb;
+  return guard([&] {
+    require(A != nullptr, "spmv: Matrix is NULL");
+    require(x != nullptr && y != nullptr, "spmv: vector array is NULL");
+    require(A->dtype == SPMV_FLOAT64 || A->dtype == SPMV_FLOAT32,
+            "spmv: only float64 and float32 products are implemented");
+    const DevCsr& C = A->fwd;
+    const size_t es = dtype_size(A->dtype);
+    SpmvArgs a;
+    a.nparts = int(C.parts.size());
+    int64_t blocks = 0;
+    for (int p = 0; p < a.nparts; ++p) {
+      const DevPart& D = C.parts[p];
+      const int64_t nb = (int64_t(D.nrows) + D.nnz + TILE - 1) / TILE;
+      PartArg& P = a.part[p];
+      P.rowptr = C.rowptr.as<int32_t>() + D.rp_off;
+      P.cols = C.cols.as<int32_t>() + D.nz_off;
+      P.vals = static_cast<const char*>(C.vals.ptr) + D.nz_off * es;
+      P.x = x[p];
+      P.y = y[p];
+      P.xown = nullptr;
+      P.nrows = D.nrows;
+      P.block_begin = int32_t(std::min<int64_t>(blocks, NOALLOC_MAX_TILES));
+      P.nblocks = int32_t(std::min<int64_t>(nb, NOALLOC_MAX_TILES));
+      P.ntiles = P.nblocks;
+      blocks += nb;
+    }
+    if (blocks > NOALLOC_MAX_TILES)
+      fail(SPMV_ERROR_INVALID_ARGUMENT,
+           "spmv_matrix_mult_noalloc: rows + nonzeros over all ranks (" +
+               std::to_string(blocks) + " tiles of 2048) exceed the maximum of " +
+               std::to_string(NOALLOC_MAX_TILES) + " tiles (33554432 items)");
+    a.nblocks = int(blocks);
+    A->comm->require_device();
+    DeviceGuard dg(A->comm->device);
+    if (blocks == 0) return;
+    unsigned char* base = static_cast<unsigned char*>(noalloc_scratch(A->comm->device));
+    int* crow = reinterpret_cast<int*>(base);
+    cudaStream_t s = A->comm->stream;
+    // Every CTA writes its carry slot before the fix-up reads it, so the
+    // array needs no clearing between calls.
+    if (A->dtype == SPMV_FLOAT64) {
+      double* cval = reinterpret_cast<double*>(base + NOALLOC_VAL_OFFSET);
+      merge_kernel<double><<<int(blocks), MBS, 0, s>>>(a, crow, cval);
+      merge_fixup<double><<<int((blocks + 255) / 256), 256, 0, s>>>(a, crow, cval,
+                                                                    int(blocks));
+    } else {
+      float* cval = reinterpret_cast<float*>(base + NOALLOC_VAL_OFFSET);
+      merge_kernel<float><<<int(blocks), MBS, 0, s>>>(a, crow, cval);
+      merge_fixup<float><<<int((blocks + 255) / 256), 256, 0, s>>>(a, crow, cval,
+                                                                   int(blocks));
+    }
+    SPMVB_CUDA(cudaGetLastError());
+  });
+}
