@@ -320,11 +320,14 @@ def run_ours(args, world, rank, local):
     kb = kernel_bytes(n, nnz, P, g)
     achieved = kb / t_mult / 1e9
     sb = spmv_bytes(n, nnz, P, g)
+    kname, kwidth, kblock = M.get_kernel()
+    kernel_fn = {"sell": "spmv_sell_kernel", "vector": "spmv_vector_kernel",
+                 "merge": "merge_kernel"}.get(kname, kname)
     traffic = None
     tp = ROOT / "profiles" / "traffic.json"
     if tp.exists():
         try:
-            traffic = json.loads(tp.read_text()).get("spmv_vector_kernel_c2")
+            traffic = json.loads(tp.read_text()).get(f"{kernel_fn}_c2")
         except Exception:
             traffic = None
 
@@ -354,7 +357,8 @@ def run_ours(args, world, rank, local):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": src, "traffic": traffic,
-                         "kernel": "spmv_vector_kernel (Matrix::mult, 8 ranks, one launch)",
+                         "kernel": f"{kernel_fn} width={kwidth} block={kblock} "
+                                   "(Matrix::mult, 8 ranks, one launch)",
                          "bytes_per_launch": kb, "us_per_launch": t_mult * 1e6},
             "spmv": {"update_plus_mult_gbs": sb / t_pair / 1e9,
                      "update_plus_mult_us": t_pair * 1e6, "bytes": sb,

@@ -67,7 +67,8 @@ typedef enum spmv_memory {
 typedef enum spmv_kernel {
   SPMV_KERNEL_AUTO = 0,   /* chosen from row-length statistics          */
   SPMV_KERNEL_VECTOR = 1, /* vector CSR: a W-lane group per row          */
-  SPMV_KERNEL_MERGE = 2   /* merge-path, load balanced for skewed rows   */
+  SPMV_KERNEL_MERGE = 2,  /* merge-path, load balanced for skewed rows   */
+  SPMV_KERNEL_SELL = 3    /* sliced ELLPACK (32-row slices), warp per slice */
 } spmv_kernel;
 
 /* Fields of the communication pattern of one rank of an L2GMap.  They are
@@ -218,8 +219,9 @@ int spmv_matrix_set_values(spmv_matrix A, spmv_memory memory,
  *    kernel. */
 int spmv_matrix_mult_noalloc(spmv_matrix A, const void* const* x,
                              void* const* y);
-/* Kernel choice.  width: lanes per row for SPMV_KERNEL_VECTOR (1..32, power
- * of two; 0 = from statistics); block: threads per CTA (0 = default). */
+/* Kernel choice.  width: lanes per row for SPMV_KERNEL_VECTOR, or loads in
+ * flight per lane for SPMV_KERNEL_SELL (1..32, power of two; 0 = from
+ * statistics); block: threads per CTA (0 = default). */
 int spmv_matrix_set_kernel(spmv_matrix A, spmv_kernel kernel, int width,
                            int block);
 int spmv_matrix_get_kernel(spmv_matrix A, spmv_kernel* kernel, int* width,
@@ -253,6 +255,74 @@ int spmv_cg(spmv_matrix A, spmv_memory memory, const double* const* b,
 int spmv_cg_ex(spmv_matrix A, spmv_memory memory, const double* const* b,
                const int64_t* b_rows, double* const* x, int max_its,
                double rtol, spmv_cg_info* info);
+
+/* ------------------------------------------------------------------------ */
+/* Mixed-precision CG (no counterpart in the reference; builds on spmv::cg)   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct spmv_ir_info {
+  int iterations;   /* inner FP32 CG iterations                             */
+  int refinements;  /* FP64 true-residual recomputations                    */
+  int status;       /* SPMV_SUCCESS or SPMV_ERROR_BREAKDOWN                 */
+  int converged;    /* 1 if ||b - A x|| / ||b|| < rtol was confirmed in FP64 */
+  double relres;    /* that FP64 relative residual, at the last refinement  */
+} spmv_ir_info;
+
+/* Solves A x = b (A FP64, SPD) to ||b - A x|| / ||b|| < rtol, checked in FP64,
+ * with FP32 inner CG iterations on an FP32 copy of A (made on first use) and
+ * FP64 refinement: FP64 solution, FP64 true residual b - A x, FP64 dot-product
+ * accumulation and FP64 alpha/beta.  Arguments as spmv_cg; max_its bounds the
+ * inner iterations.  Runs as one CUDA graph launch. */
+int spmv_cg_mixed(spmv_matrix A, spmv_memory memory, const double* const* b,
+                  const int64_t* b_rows, double* const* x, int max_its,
+                  double rtol, spmv_ir_info* info);
+
+/* ------------------------------------------------------------------------ */
+/* Batched solves (no counterpart in the reference; builds on spmv::cg)      */
+/* ------------------------------------------------------------------------ */
+
+typedef struct spmv_batch_s* spmv_batch;
+
+typedef struct spmv_batch_info {
+  int iterations;   /* inner FP32 CG iterations of this system               */
+  int refinements;  /* FP64 true-residual recomputations                     */
+  int status;       /* SPMV_SUCCESS or SPMV_ERROR_BREAKDOWN                  */
+  int converged;    /* 1 if ||b - A x|| / ||b|| < rtol was confirmed in FP64  */
+  double relres;    /* that FP64 relative residual                           */
+} spmv_batch_info;
+
+/* nsys independent SPD systems of sizes n[i] (square CSR blocks, FP64 values;
+ * an FP32 copy is made for the inner iterations).  Copies in. */
+int spmv_batch_create(spmv_comm comm, int nsys, const int32_t* n,
+                      const int32_t* const* rowptr,
+                      const int32_t* const* colind,
+                      const double* const* values, spmv_batch* batch);
+int spmv_batch_destroy(spmv_batch batch);
+/* CTAs (on different SMs, one thread-block cluster) that share one system:
+ * 1, 2, 4 or 8 (default 1). */
+int spmv_batch_set_cluster(spmv_batch batch, int cluster);
+/* Solves every system A_i x_i = b_i to ||b_i - A_i x_i|| / ||b_i|| < rtol
+ * (checked in FP64) in one persistent launch: FP32 inner CG iterations with
+ * FP64 refinement, as spmv_cg_mixed, one system per thread-block cluster from
+ * a work queue ordered largest first.  b[nsys], x[nsys]; info[nsys] may be
+ * NULL.  max_its bounds each system's inner iterations. */
+int spmv_batch_solve(spmv_batch batch, spmv_memory memory,
+                     const double* const* b, double* const* x, int max_its,
+                     double rtol, spmv_batch_info* info);
+
+/* ------------------------------------------------------------------------ */
+/* Adjoint of x = A^{-1} b (no counterpart in the reference)                 */
+/* ------------------------------------------------------------------------ */
+
+/* out[r][k] = scale * lambda[r][row(k)] * x[r][col(k)] for every stored entry
+ * k of rank r's block, in the block's entry order.  With lambda the adjoint
+ * solution (A^T lambda = dL/dx; spmv_cg on A for symmetric A) and scale = -1
+ * this is dL/dA on A's sparsity pattern; dL/db is lambda itself.  lambda[r]
+ * has nrows[r] entries, x[r] ncols[r] (owned then ghosts: update it first),
+ * out[r] nnz[r]; all of the matrix dtype. */
+int spmv_matrix_sample_outer(spmv_matrix A, spmv_memory memory, double scale,
+                             const void* const* lambda, const void* const* x,
+                             void* const* out);
 
 #ifdef __cplusplus
 }

@@ -22,7 +22,7 @@ FLOAT64, FLOAT32, COMPLEX64, COMPLEX128 = 0, 1, 2, 3
 # spmv_memory
 MEMORY_HOST, MEMORY_DEVICE = 0, 1
 # spmv_kernel
-KERNEL_AUTO, KERNEL_VECTOR, KERNEL_MERGE = 0, 1, 2
+KERNEL_AUTO, KERNEL_VECTOR, KERNEL_MERGE, KERNEL_SELL = 0, 1, 2, 3
 # spmv_pattern_field
 PATTERN_FIELDS = {"neighbours": 0, "send_count": 1, "recv_count": 2,
                   "send_offset": 3, "recv_offset": 4, "indexbuf": 5}
@@ -42,6 +42,14 @@ class SpmvError(RuntimeError):
 class CgInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("status", C.c_int),
                 ("rnorm0", C.c_double), ("rnorm", C.c_double)]
+
+
+class IrInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("refinements", C.c_int),
+                ("status", C.c_int), ("converged", C.c_int), ("relres", C.c_double)]
+
+
+BatchInfo = IrInfo  # same layout as spmv_batch_info
 
 
 _p = C.c_void_p
@@ -93,6 +101,13 @@ _SIGS = {
                 C.POINTER(_int)],
     "spmv_cg_ex": [_p, _int, _pp, C.POINTER(_i64), _pp, _int, C.c_double,
                    C.POINTER(CgInfo)],
+    "spmv_cg_mixed": [_p, _int, _pp, C.POINTER(_i64), _pp, _int, C.c_double,
+                      C.POINTER(IrInfo)],
+    "spmv_matrix_sample_outer": [_p, _int, C.c_double, _pp, _pp, _pp],
+    "spmv_batch_create": [_p, _int, C.POINTER(_i32), _pp, _pp, _pp, C.POINTER(_p)],
+    "spmv_batch_destroy": [_p],
+    "spmv_batch_set_cluster": [_p, _int],
+    "spmv_batch_solve": [_p, _int, _pp, _pp, _int, C.c_double, C.POINTER(IrInfo)],
 }
 
 _lib = None

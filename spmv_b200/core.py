@@ -29,6 +29,32 @@ def _is_torch(v) -> bool:
     return type(v).__module__.startswith("torch")
 
 
+class _Fence:
+    """Orders library work after and before torch work on device tensors.
+
+    The communicator's CUDA stream is not torch's current stream, so on entry
+    the library stream waits for work already queued on torch's stream (that
+    produced the inputs), and on exit torch's stream waits for the library's
+    work (that produces the outputs).  Both waits are device-side events; the
+    host does not block."""
+
+    def __init__(self, comm, device: bool):
+        self.comm = comm if device else None
+
+    def __enter__(self):
+        if self.comm is not None:
+            import torch
+            self.torch_stream = torch.cuda.current_stream(self.comm.device)
+            self.lib_stream = self.comm.torch_stream()
+            self.lib_stream.wait_stream(self.torch_stream)
+        return self
+
+    def __exit__(self, *exc):
+        if self.comm is not None:
+            self.torch_stream.wait_stream(self.lib_stream)
+        return False
+
+
 def _vec_info(vecs: Sequence):
     """(memory kind, dtype code, addresses) of a per-rank vector list."""
     if len(vecs) == 0:
@@ -86,6 +112,17 @@ class Comm:
 
     def synchronize(self) -> None:
         call("spmv_comm_synchronize", self._h)
+
+    def torch_stream(self):
+        """The communicator's stream as a torch.cuda.ExternalStream."""
+        if getattr(self, "_ts", None) is None:
+            import torch
+            self._ts = torch.cuda.ExternalStream(self.stream,
+                                                 device=torch.device("cuda", self.device))
+        return self._ts
+
+    def fence(self, vecs) -> "_Fence":
+        return _Fence(self, bool(vecs) and _is_torch(vecs[0]))
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
@@ -169,12 +206,14 @@ class L2GMap:
     def update(self, vecs: Sequence) -> None:
         """L2GMap::update (L2GMap.cpp:126-150) on all ranks' vectors, in place."""
         mem, dt, ptrs = _vec_info(vecs)
-        call("spmv_l2gmap_update", self._h, dt, mem, ptr_array(ptrs))
+        with self.comm.fence(vecs):
+            call("spmv_l2gmap_update", self._h, dt, mem, ptr_array(ptrs))
 
     def reverse_update(self, vecs: Sequence) -> None:
         """L2GMap::reverse_update (L2GMap.cpp:152-170), in place."""
         mem, dt, ptrs = _vec_info(vecs)
-        call("spmv_l2gmap_reverse_update", self._h, dt, mem, ptr_array(ptrs))
+        with self.comm.fence(vecs):
+            call("spmv_l2gmap_reverse_update", self._h, dt, mem, ptr_array(ptrs))
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
@@ -260,17 +299,18 @@ class Matrix:
 
     def set_values(self, values: Sequence) -> None:
         mem, dt, ptrs = _vec_info(values)
-        call("spmv_matrix_set_values", self._h, mem, ptr_array(ptrs))
+        with self.comm.fence(values):
+            call("spmv_matrix_set_values", self._h, mem, ptr_array(ptrs))
 
     def set_kernel(self, kernel: str = "auto", width: int = 0, block: int = 0) -> None:
         k = {"auto": _lib.KERNEL_AUTO, "vector": _lib.KERNEL_VECTOR,
-             "merge": _lib.KERNEL_MERGE}[kernel]
+             "merge": _lib.KERNEL_MERGE, "sell": _lib.KERNEL_SELL}[kernel]
         call("spmv_matrix_set_kernel", self._h, k, width, block)
 
     def get_kernel(self):
         k, w, b = C.c_int(), C.c_int(), C.c_int()
         call("spmv_matrix_get_kernel", self._h, C.byref(k), C.byref(w), C.byref(b))
-        return {0: "auto", 1: "vector", 2: "merge"}[k.value], w.value, b.value
+        return {0: "auto", 1: "vector", 2: "merge", 3: "sell"}[k.value], w.value, b.value
 
     def _alloc_like(self, x0, lens):
         if _is_torch(x0):
@@ -283,7 +323,8 @@ class Matrix:
         mem, dt, ptrs = _vec_info(x)
         y = out if out is not None else self._alloc_like(x[0], self.nrows)
         _, _, yptrs = _vec_info(y)
-        call("spmv_matrix_mult", self._h, mem, ptr_array(ptrs), ptr_array(yptrs))
+        with self.comm.fence(x):
+            call("spmv_matrix_mult", self._h, mem, ptr_array(ptrs), ptr_array(yptrs))
         return y
 
     __mul__ = mult
@@ -293,8 +334,24 @@ class Matrix:
         mem, dt, ptrs = _vec_info(x)
         y = out if out is not None else self._alloc_like(x[0], self.ncols)
         _, _, yptrs = _vec_info(y)
-        call("spmv_matrix_transpmult", self._h, mem, ptr_array(ptrs), ptr_array(yptrs))
+        with self.comm.fence(x):
+            call("spmv_matrix_transpmult", self._h, mem, ptr_array(ptrs),
+                 ptr_array(yptrs))
         return y
+
+    def sample_outer(self, lam: Sequence, x: Sequence, scale: float = -1.0,
+                     out: Optional[List] = None) -> List:
+        """out[r][k] = scale * lam[r][row(k)] * x[r][col(k)] on every stored
+        entry (dL/dA on A's pattern for scale = -1, lam the adjoint)."""
+        mem, dt, lptrs = _vec_info(lam)
+        _, _, xptrs = _vec_info(x)
+        if out is None:
+            out = self._alloc_like(lam[0], [self.nnz(r) for r in range(self.comm.size)])
+        _, _, optrs = _vec_info(out)
+        with self.comm.fence(lam):
+            call("spmv_matrix_sample_outer", self._h, mem, float(scale),
+                 ptr_array(lptrs), ptr_array(xptrs), ptr_array(optrs))
+        return out
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
@@ -323,9 +380,78 @@ def cg(comm: Comm, A: Matrix, b: Sequence, max_its: int, rtol: float,
     _, _, xptrs = _vec_info(x)
     rows = (C.c_int64 * comm.size)(*[len(v) for v in b])
     ci = _lib.CgInfo()
-    st = _lib.lib().spmv_cg_ex(A.handle, mem, ptr_array(bptrs), rows, ptr_array(xptrs),
-                               int(max_its), float(rtol), C.byref(ci))
+    with comm.fence(b):
+        st = _lib.lib().spmv_cg_ex(A.handle, mem, ptr_array(bptrs), rows,
+                                   ptr_array(xptrs), int(max_its), float(rtol),
+                                   C.byref(ci))
     _lib.check(st)
     if info:
         return x, ci.iterations, ci
     return x, ci.iterations
+
+
+def cg_mixed(comm: Comm, A: Matrix, b: Sequence, max_its: int, rtol: float,
+             x: Optional[List] = None):
+    """Mixed-precision CG (FP32 inner iterations, FP64 refinement) to
+    ||b - A x|| / ||b|| < rtol confirmed in FP64.  Returns (x, IrInfo)."""
+    if comm is not A.comm:
+        raise SpmvError(_lib.ERROR_INVALID_ARGUMENT, "spmv::cg - Error: comm mismatch")
+    mem, dt, bptrs = _vec_info(b)
+    cm = A.col_map()
+    if x is None:
+        x = A._alloc_like(b[0], [cm.vec_len(r) for r in range(comm.size)])
+    _, _, xptrs = _vec_info(x)
+    rows = (C.c_int64 * comm.size)(*[len(v) for v in b])
+    info = _lib.IrInfo()
+    with comm.fence(b):
+        st = _lib.lib().spmv_cg_mixed(A.handle, mem, ptr_array(bptrs), rows,
+                                      ptr_array(xptrs), int(max_its), float(rtol),
+                                      C.byref(info))
+    _lib.check(st)
+    return x, info
+
+
+class Batch:
+    """Many independent SPD systems (one CSR each) solved together by
+    spmv_batch_solve: one persistent launch, FP32 inner CG with FP64
+    refinement, largest systems first."""
+
+    def __init__(self, comm: Comm, systems, cluster: int = 1):
+        self.comm = comm
+        self._rp = [np.ascontiguousarray(s[0], np.int32) for s in systems]
+        self._ci = [np.ascontiguousarray(s[1], np.int32) for s in systems]
+        self._va = [np.ascontiguousarray(s[2], np.float64) for s in systems]
+        self.n = [len(rp) - 1 for rp in self._rp]
+        ns = len(systems)
+        h = C.c_void_p()
+        call("spmv_batch_create", comm.handle, ns, (C.c_int32 * max(ns, 1))(*self.n),
+             ptr_array([a.ctypes.data for a in self._rp]),
+             ptr_array([a.ctypes.data for a in self._ci]),
+             ptr_array([a.ctypes.data for a in self._va]), C.byref(h))
+        self._h = h
+        self.set_cluster(cluster)
+
+    def set_cluster(self, cluster: int) -> None:
+        call("spmv_batch_set_cluster", self._h, int(cluster))
+
+    def solve(self, b: Sequence, max_its: int, rtol: float, x: Optional[List] = None):
+        mem, dt, bptrs = _vec_info(b)
+        if x is None:
+            x = [np.empty_like(v) if not _is_torch(v) else v.new_empty(v.shape) for v in b]
+        _, _, xptrs = _vec_info(x)
+        info = (_lib.BatchInfo * max(len(b), 1))()
+        with self.comm.fence(b):
+            call("spmv_batch_solve", self._h, mem, ptr_array(bptrs), ptr_array(xptrs),
+                 int(max_its), float(rtol), info)
+        return x, list(info)[:len(b)]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.lib().spmv_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -97,6 +97,9 @@ void upload_csr(spmv_matrix A) {
   C.nz_total = nz + 4;  // room for the masked tail of the last 16-byte load
   C.mean_row = rows > 0 ? double(nnz_all) / double(rows) : 0.0;
   C.max_row = maxr;
+  C.sell_padded = 0;
+  for (int r = 0; r < P; ++r)
+    C.sell_padded += sell_padded_size(A->h_rowptr[r], A->nrows[r], nullptr);
   if (A->comm->device < 0) return;
   DeviceGuard dg(A->comm->device);
   C.rowptr.reserve(sizeof(int32_t) * std::max<int64_t>(C.rp_total, 1));
@@ -244,6 +247,8 @@ void product(spmv_matrix A, bool transpose, spmv_memory memory,
           "spmv: unknown memory kind");
   DeviceGuard dg(comm->device);
   if (transpose) build_transpose(A);
+  if (!transpose && pick_kernel(A->kernel, A->fwd) == SPMV_KERNEL_SELL)
+    build_sell(A, A->fwd, comm->stream);
   const DevCsr& C = transpose ? A->trn : A->fwd;
   const int P = comm->size;
   const size_t es = dtype_size(A->dtype);
@@ -330,6 +335,76 @@ void halo(spmv_l2gmap map, bool reverse, spmv_dtype dtype, spmv_memory memory,
   for (int r = 0; r < P; ++r)
     if (len[r] > 0)
       SPMVB_CUDA(cudaMemcpyAsync(vecs[r], dv[r], len[r] * es, cudaMemcpyDeviceToHost, s));
+  SPMVB_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+}  // namespace spmvb
+
+namespace spmvb {
+namespace {
+
+// Checks shared by spmv_cg and spmv_cg_mixed (cg.cpp:22-28 and the layout
+// the fused-halo solve needs).
+void check_solve_args(spmv_matrix A, spmv_memory memory, const double* const* b,
+                      const int64_t* b_rows, double* const* x) {
+  check_mat(A);
+  require(A->dtype == SPMV_FLOAT64, "spmv::cg - Error: A must be float64");
+  spmv_l2gmap rm = A->row_map, cm = A->col_map;
+  require(rm != nullptr && cm != nullptr, "spmv::cg - Error: A needs row and column maps");
+  const int P = A->comm->size;
+  for (int r = 0; r < P; ++r)
+    if (!rm->rank[r].ghosts.empty())
+      fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv::cg - Error: A.row_map() has ghost entries");
+  if (b_rows)
+    for (int r = 0; r < P; ++r)
+      if (b_rows[r] != rm->rank[r].local_size)
+        fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv::cg - Error: b.rows() != A.rows()");
+  // p.head(M) (cg.cpp:41) needs the owned column range to be the row range.
+  for (int r = 0; r < P; ++r)
+    require(cm->rank[r].local_size == rm->rank[r].local_size,
+            "spmv::cg - Error: column map local sizes differ from row map");
+  require(b != nullptr && x != nullptr, "spmv::cg - Error: NULL vector array");
+  require(memory == SPMV_MEMORY_HOST || memory == SPMV_MEMORY_DEVICE,
+          "spmv: unknown memory kind");
+  A->comm->require_device();
+}
+
+// Rank vectors b[r] into the global-layout device vector.
+void copy_rhs_in(spmv_matrix A, spmv_memory memory, const double* const* b, double* db) {
+  spmv_l2gmap rm = A->row_map;
+  cudaStream_t s = A->comm->stream;
+  const cudaMemcpyKind k = memory == SPMV_MEMORY_HOST ? cudaMemcpyHostToDevice
+                                                      : cudaMemcpyDeviceToDevice;
+  for (int r = 0; r < A->comm->size; ++r) {
+    const int64_t M = rm->rank[r].local_size;
+    if (M == 0) continue;
+    require(b[r] != nullptr, "spmv::cg - Error: b is NULL");
+    SPMVB_CUDA(cudaMemcpyAsync(db + rm->ranges[r], b[r], M * sizeof(double), k, s));
+  }
+}
+
+// Global-layout solution into the rank vectors x[r] (ghost tail zero).
+void copy_solution_out(spmv_matrix A, spmv_memory memory, const double* dx,
+                       double* const* x) {
+  spmv_l2gmap rm = A->row_map, cm = A->col_map;
+  cudaStream_t s = A->comm->stream;
+  const cudaMemcpyKind k = memory == SPMV_MEMORY_HOST ? cudaMemcpyDeviceToHost
+                                                      : cudaMemcpyDeviceToDevice;
+  for (int r = 0; r < A->comm->size; ++r) {
+    const int64_t M = rm->rank[r].local_size;
+    const int64_t G = int64_t(cm->rank[r].ghosts.size());
+    if (M + G == 0) continue;
+    require(x[r] != nullptr, "spmv::cg - Error: x is NULL");
+    if (M > 0)
+      SPMVB_CUDA(cudaMemcpyAsync(x[r], dx + rm->ranges[r], M * sizeof(double), k, s));
+    if (G > 0) {
+      if (memory == SPMV_MEMORY_HOST)
+        std::fill(x[r] + M, x[r] + M + G, 0.0);
+      else
+        SPMVB_CUDA(cudaMemsetAsync(x[r] + M, 0, G * sizeof(double), s));
+    }
+  }
   SPMVB_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -713,10 +788,62 @@ int spmv_matrix_set_values(spmv_matrix A, spmv_memory memory,
         SPMVB_CUDA(cudaMemcpy(A->fwd.vals.as<char>() + A->fwd.parts[r].nz_off * es,
                               A->h_vals[r].data(), nnz * es, cudaMemcpyHostToDevice));
     }
-    // Derived copies are rebuilt on next use.
+    // Derived copies are rebuilt on next use (the mixed solver's graph holds
+    // the FP32 copy's address, so it goes too).
     A->trn_built = false;
     A->trn = DevCsr{};
+    A->ir.reset();
     A->fwd.vals32.release();
+    if (A->comm->device >= 0) refresh_sell_values(A);
+  });
+}
+
+int spmv_matrix_sample_outer(spmv_matrix A, spmv_memory memory, double scale,
+                             const void* const* lambda, const void* const* x,
+                             void* const* out) {
+  return guard([&] {
+    check_mat(A);
+    spmv_comm comm = A->comm;
+    comm->require_device();
+    require(lambda && x && out, "spmv: vector array is NULL");
+    require(A->dtype == SPMV_FLOAT64 || A->dtype == SPMV_FLOAT32,
+            "spmv: only float64 and float32 matrices are implemented");
+    DeviceGuard dg(comm->device);
+    cudaStream_t s = comm->stream;
+    if (memory == SPMV_MEMORY_DEVICE) {
+      launch_sample_outer(A, scale, lambda, x, out, s);
+      return;
+    }
+    require(memory == SPMV_MEMORY_HOST, "spmv: unknown memory kind");
+    const int P = comm->size;
+    const size_t es = dtype_size(A->dtype);
+    std::vector<int64_t> lens;  // lambda[P], x[P], out[P]
+    for (int r = 0; r < P; ++r) lens.push_back(A->nrows[r]);
+    for (int r = 0; r < P; ++r) lens.push_back(A->ncols[r]);
+    for (int r = 0; r < P; ++r) lens.push_back(A->h_rowptr[r][A->nrows[r]]);
+    Staging st;
+    st.layout(lens, es);
+    comm->stage_in.reserve(std::max<int64_t>(st.total, 256));
+    std::vector<const void*> dl(P), dx(P);
+    std::vector<void*> dout(P);
+    char* base = comm->stage_in.as<char>();
+    for (int r = 0; r < P; ++r) {
+      dl[r] = base + st.off[r];
+      dx[r] = base + st.off[P + r];
+      dout[r] = base + st.off[2 * P + r];
+      if (lens[r] > 0)
+        SPMVB_CUDA(cudaMemcpyAsync(const_cast<void*>(dl[r]), lambda[r], lens[r] * es,
+                                   cudaMemcpyHostToDevice, s));
+      if (lens[P + r] > 0)
+        SPMVB_CUDA(cudaMemcpyAsync(const_cast<void*>(dx[r]), x[r], lens[P + r] * es,
+                                   cudaMemcpyHostToDevice, s));
+    }
+    launch_sample_outer(A, scale, dl.data(), dx.data(), dout.data(), s);
+    for (int r = 0; r < P; ++r)
+      if (lens[2 * P + r] > 0)
+        SPMVB_CUDA(cudaMemcpyAsync(out[r], dout[r], lens[2 * P + r] * es,
+                                   cudaMemcpyDeviceToHost, s));
+    SPMVB_CUDA(cudaStreamSynchronize(s));
   });
 }
 
@@ -725,16 +852,19 @@ int spmv_matrix_set_kernel(spmv_matrix A, spmv_kernel kernel, int width,
   return guard([&] {
     check_mat(A);
     require(kernel == SPMV_KERNEL_AUTO || kernel == SPMV_KERNEL_VECTOR ||
-                kernel == SPMV_KERNEL_MERGE,
+                kernel == SPMV_KERNEL_MERGE || kernel == SPMV_KERNEL_SELL,
             "spmv: unknown kernel");
     require(width == 0 || (width >= 1 && width <= 32 && (width & (width - 1)) == 0),
             "spmv: width must be 0 or 1..32, a power of two");
+    require(kernel != SPMV_KERNEL_SELL || width <= 16,
+            "spmv: SELL width (loads in flight per lane) must be 1..16");
     require(block == 0 || block == 128 || block == 256 || block == 512,
             "spmv: block must be 0, 128, 256 or 512");
     A->kernel = kernel;
     A->width = width;
     A->block = block;
     A->cg.reset();  // graphs bake the kernel choice in
+    A->ir.reset();
   });
 }
 
@@ -744,7 +874,10 @@ int spmv_matrix_get_kernel(spmv_matrix A, spmv_kernel* kernel, int* width,
     check_mat(A);
     require(kernel && width && block, "spmv: NULL output");
     *kernel = pick_kernel(A->kernel, A->fwd);
-    *width = A->width > 0 ? A->width : auto_width(A->fwd.mean_row, A->dtype);
+    if (A->width > 0)
+      *width = A->width;
+    else
+      *width = *kernel == SPMV_KERNEL_SELL ? 8 : auto_width(A->fwd.mean_row, A->dtype);
     *block = A->block > 0 ? A->block : 256;
   });
 }
@@ -754,65 +887,35 @@ int spmv_cg_ex(spmv_matrix A, spmv_memory memory, const double* const* b,
                const int64_t* b_rows, double* const* x, int max_its,
                double rtol, spmv_cg_info* info) {
   return guard([&] {
-    check_mat(A);
-    require(A->dtype == SPMV_FLOAT64, "spmv::cg - Error: A must be float64");
-    spmv_l2gmap rm = A->row_map, cm = A->col_map;
-    require(rm != nullptr && cm != nullptr,
-            "spmv::cg - Error: A needs row and column maps");
-    const int P = A->comm->size;
-    // cg.cpp:22-23 and 27-28, checked for every rank.
-    for (int r = 0; r < P; ++r)
-      if (!rm->rank[r].ghosts.empty())
-        fail(SPMV_ERROR_INVALID_ARGUMENT,
-             "spmv::cg - Error: A.row_map() has ghost entries");
-    if (b_rows)
-      for (int r = 0; r < P; ++r)
-        if (b_rows[r] != rm->rank[r].local_size)
-          fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv::cg - Error: b.rows() != A.rows()");
-    // p.head(M) (cg.cpp:41) needs the owned column range to be the row range.
-    for (int r = 0; r < P; ++r)
-      require(cm->rank[r].local_size == rm->rank[r].local_size,
-              "spmv::cg - Error: column map local sizes differ from row map");
-    require(b != nullptr && x != nullptr, "spmv::cg - Error: NULL vector array");
-    require(memory == SPMV_MEMORY_HOST || memory == SPMV_MEMORY_DEVICE,
-            "spmv: unknown memory kind");
-    A->comm->require_device();
+    check_solve_args(A, memory, b, b_rows, x);
     DeviceGuard dg(A->comm->device);
-    cudaStream_t s = A->comm->stream;
-    double* db = cg_rhs(A);
-    double* dx = cg_solution(A);
-    const cudaMemcpyKind in = memory == SPMV_MEMORY_HOST ? cudaMemcpyHostToDevice
-                                                         : cudaMemcpyDeviceToDevice;
-    const cudaMemcpyKind outk = memory == SPMV_MEMORY_HOST ? cudaMemcpyDeviceToHost
-                                                           : cudaMemcpyDeviceToDevice;
-    for (int r = 0; r < P; ++r) {
-      const int64_t M = rm->rank[r].local_size;
-      if (M == 0) continue;
-      require(b[r] != nullptr, "spmv::cg - Error: b is NULL");
-      SPMVB_CUDA(cudaMemcpyAsync(db + rm->ranges[r], b[r], M * sizeof(double), in, s));
-    }
+    copy_rhs_in(A, memory, b, cg_rhs(A));
     spmv_cg_info local{};
     cg_run(A, max_its, rtol, &local);
-    for (int r = 0; r < P; ++r) {
-      const int64_t M = rm->rank[r].local_size;
-      const int64_t G = int64_t(cm->rank[r].ghosts.size());
-      if (M + G == 0) continue;
-      require(x[r] != nullptr, "spmv::cg - Error: x is NULL");
-      if (M > 0)
-        SPMVB_CUDA(cudaMemcpyAsync(x[r], dx + rm->ranges[r], M * sizeof(double), outk, s));
-      if (G > 0) {
-        if (memory == SPMV_MEMORY_HOST)
-          std::fill(x[r] + M, x[r] + M + G, 0.0);
-        else
-          SPMVB_CUDA(cudaMemsetAsync(x[r] + M, 0, G * sizeof(double), s));
-      }
-    }
-    SPMVB_CUDA(cudaStreamSynchronize(s));
+    copy_solution_out(A, memory, cg_solution(A), x);
     if (info) *info = local;
     if (local.status == SPMV_ERROR_BREAKDOWN)
       fail(SPMV_ERROR_BREAKDOWN,
            "spmv::cg - Error: breakdown, p.Ap is zero or not finite at iteration " +
                std::to_string(local.iterations));
+  });
+}
+
+int spmv_cg_mixed(spmv_matrix A, spmv_memory memory, const double* const* b,
+                  const int64_t* b_rows, double* const* x, int max_its,
+                  double rtol, spmv_ir_info* info) {
+  return guard([&] {
+    check_solve_args(A, memory, b, b_rows, x);
+    DeviceGuard dg(A->comm->device);
+    copy_rhs_in(A, memory, b, ir_rhs(A));
+    spmv_ir_info local{};
+    ir_run(A, max_its, rtol, &local);
+    copy_solution_out(A, memory, ir_solution(A), x);
+    if (info) *info = local;
+    if (local.status == SPMV_ERROR_BREAKDOWN)
+      fail(SPMV_ERROR_BREAKDOWN,
+           "spmv::cg - Error: breakdown in the mixed-precision solve after " +
+               std::to_string(local.iterations) + " iterations");
   });
 }
 

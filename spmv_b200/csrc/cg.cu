@@ -36,6 +36,7 @@ struct CgState {
 struct CgWorkspace {
   int64_t n = 0;
   int W = 0, BS = 256;
+  bool sell = false;  // K1 over the SELL-32 copy (W = loads per lane)
   spmvb::DevBuf b, x, r, p, y, partials, state;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -90,6 +91,36 @@ __global__ void __launch_bounds__(EW_BS)
     const bool go = st->kmax > 0 && total > 0.0 && isfinite(total);
     cudaGraphSetConditional(h, go ? 1u : 0u);
   }
+}
+
+// K1 epilogue: the grid-wide p.y, alpha and the breakdown test.
+template <int BS>
+__device__ __forceinline__ void cg_dot_finish(double acc, const CgPtrs& c,
+                                              double* smem) {
+  const double part = block_sum<BS>(acc, smem);
+  double total;
+  if (grid_sum<BS>(part, c.partials, &c.st->ticket1, &total, smem) &&
+      threadIdx.x == 0) {
+    CgState* st = c.st;
+    st->pdoty = total;
+    if (total == 0.0 || !isfinite(total)) st->status = SPMV_ERROR_BREAKDOWN;
+    st->alpha = st->rnorm_old / total;
+  }
+}
+
+// K1 over the SELL-32 copy (U loads in flight per lane).
+template <int U, int BS>
+__global__ void __launch_bounds__(BS)
+    cg_spmv_dot_sell(const __grid_constant__ SpmvArgs a, const CgPtrs c,
+                     cudaGraphConditionalHandle h) {
+  __shared__ double smem[32];
+  if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
+  double acc = 0.0;
+  sell_for_rows<double, BS, U>(a, [&](const PartArg& P, int row, double sum) {
+    static_cast<double*>(P.y)[row] = sum;
+    acc += static_cast<const double*>(P.xown)[row] * sum;
+  });
+  cg_dot_finish<BS>(acc, c, smem);
 }
 
 template <int W, int BS>
@@ -170,6 +201,17 @@ DotFn dot_kernel(int W) {
   fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: width must be 1..32, a power of two");
 }
 
+DotFn dot_kernel_sell(int U) {
+  switch (U) {
+    case 1: return cg_spmv_dot_sell<1, 256>;
+    case 2: return cg_spmv_dot_sell<2, 256>;
+    case 4: return cg_spmv_dot_sell<4, 256>;
+    case 8: return cg_spmv_dot_sell<8, 256>;
+    case 16: return cg_spmv_dot_sell<16, 256>;
+  }
+  fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: SELL width must be 1, 2, 4, 8 or 16");
+}
+
 void add_kernel(cudaGraphNode_t* node, cudaGraph_t g, const cudaGraphNode_t* dep,
                 size_t ndep, void* fn, int grid, int block, void** args) {
   cudaKernelNodeParams kp{};
@@ -198,9 +240,14 @@ void build_graph(spmv_matrix A, CgWorkspace& w) {
     ys[r] = w.y.as<double>() + rm->ranges[r];
   }
   SpmvArgs sa;
-  fill_spmv_args(sa, A->fwd, A->fwd.cols_global.as<int32_t>(), sizeof(double),
-                 xs.data(), ys.data(), xown.data(), BS / W,
-                 max_blocks_for(comm->num_sms, BS));
+  if (w.sell)
+    fill_sell_args(sa, A->fwd, A->fwd.sell_cols_global.as<int32_t>(),
+                   A->fwd.sell_vals.ptr, sizeof(double), xs.data(), ys.data(),
+                   xown.data(), BS, max_blocks_for(comm->num_sms, BS));
+  else
+    fill_spmv_args(sa, A->fwd, A->fwd.cols_global.as<int32_t>(), sizeof(double),
+                   xs.data(), ys.data(), xown.data(), BS / W,
+                   max_blocks_for(comm->num_sms, BS));
   const int ew_grid = std::max(1, comm->num_sms) * (2048 / EW_BS);
   w.partials.reserve(sizeof(double) * std::max(sa.nblocks, ew_grid));
 
@@ -234,7 +281,8 @@ void build_graph(spmv_matrix A, CgWorkspace& w) {
   cudaGraphNode_t k1 = nullptr, k2 = nullptr, k3 = nullptr;
   if (sa.nblocks > 0) {
     void* args[] = {&sa, &c, &w.handle};
-    add_kernel(&k1, body, nullptr, 0, (void*)dot_kernel(W), sa.nblocks, BS,
+    add_kernel(&k1, body, nullptr, 0,
+               (void*)(w.sell ? dot_kernel_sell(W) : dot_kernel(W)), sa.nblocks, BS,
                args);
   }
   {
@@ -268,7 +316,10 @@ CgWorkspace& cg_workspace(spmv_matrix A) {
     w->y.reserve(bytes);
     w->state.reserve(sizeof(CgState));
     SPMVB_CUDA(cudaMemset(w->state.ptr, 0, sizeof(CgState)));
-    w->W = A->width > 0 ? A->width : auto_width(A->fwd.mean_row, SPMV_FLOAT64);
+    w->sell = pick_kernel(A->kernel, A->fwd) == SPMV_KERNEL_SELL;
+    if (w->sell) build_sell_global(A);
+    w->W = A->width > 0 ? A->width
+                        : (w->sell ? 8 : auto_width(A->fwd.mean_row, SPMV_FLOAT64));
     w->BS = 256;
     build_graph(A, *w);
     A->cg = std::move(w);

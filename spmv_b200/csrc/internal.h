@@ -194,6 +194,10 @@ struct DevPart {
   int64_t nnz = 0;
   int64_t rp_off = 0;   // offset of this rank's rowptr in the concatenation
   int64_t nz_off = 0;   // offset of this rank's entries (aligned to 4)
+  // SELL-32 layout of the same block (when built).
+  int64_t sl_off = 0;   // offset of this rank's slice offsets
+  int64_t sz_off = 0;   // offset of this rank's SELL entries
+  int64_t snnz = 0;     // SELL entries including padding
 };
 
 // A device CSR (all ranks concatenated) plus the derived column arrays.
@@ -206,14 +210,23 @@ struct DevCsr {
   DevBuf cols_global;   // int32: global column indices (fused-halo layout)
   DevBuf vals32;        // float copy of FP64 values (mixed precision)
   DevBuf merge_carry;   // per-CTA carries of the merge-path product
+  // SELL-32 copy (sliced ELLPACK, padding columns are -1), built when the
+  // kernel choice is SELL: slice offsets (int32, per rank relative to the
+  // rank's first SELL entry, nslices+1 each), columns, values, and the
+  // fused-halo / FP32 variants.
+  bool sell_built = false;
+  int64_t sl_total = 0, sz_total = 0;
+  DevBuf sell_off, sell_cols, sell_vals, sell_cols_global, sell_vals32;
   // Row statistics (over all ranks).
   double mean_row = 0;
   int64_t max_row = 0;
+  int64_t sell_padded = 0;   // SELL-32 entries (with padding) over all ranks
 };
 
 }  // namespace spmvb
 
 struct CgWorkspace;  // cg.cu
+struct IrWorkspace;  // ir.cu
 
 struct spmv_matrix_s {
   spmv_comm comm = nullptr;
@@ -231,6 +244,7 @@ struct spmv_matrix_s {
   spmv_kernel kernel = SPMV_KERNEL_AUTO;
   int width = 0, block = 0;
   std::unique_ptr<CgWorkspace, void (*)(CgWorkspace*)> cg{nullptr, nullptr};
+  std::unique_ptr<IrWorkspace, void (*)(IrWorkspace*)> ir{nullptr, nullptr};
 };
 
 namespace spmvb {
@@ -251,12 +265,29 @@ struct SpmvLaunch {
 };
 void launch_spmv(const SpmvLaunch& L, cudaStream_t stream);
 void launch_merge(const SpmvLaunch& L, cudaStream_t stream, DevBuf& carry);
-// Kernel family for a matrix: the caller's choice, or from row statistics
-// (merge-path when the longest row is far above the mean).
-spmv_kernel pick_kernel(spmv_kernel requested, const DevCsr& C);
+// Kernel family for a matrix: the caller's choice, or from row statistics:
+// merge-path when the longest row is far above the mean, SELL-32 when its
+// padding is small (allow_sell: the SELL copy can exist for this CSR), else
+// vector CSR.  A SELL request where SELL cannot be used gives vector CSR.
+spmv_kernel pick_kernel(spmv_kernel requested, const DevCsr& C, bool allow_sell = true);
 // Lanes per row picked from the mean row length (vector kernel).
 int auto_width(double mean_row, spmv_dtype dtype);
 int max_blocks_for(int num_sms, int BS);
+// SELL-32 layout (sell.cu): built on the device from the device CSR.
+int64_t sell_padded_size(const std::vector<int32_t>& rowptr, int32_t nrows,
+                         std::vector<int32_t>* soff);
+void build_sell(spmv_matrix A, DevCsr& C, cudaStream_t stream);
+// After new values: re-scatter them into the SELL copy (same pattern).
+void refresh_sell_values(spmv_matrix A);
+void launch_sell(const SpmvLaunch& L, const int32_t* sell_cols, cudaStream_t stream);
+// SELL copies of the fused-halo columns and of the FP32 values.
+void build_sell_global(spmv_matrix A);
+void build_sell_vals32(spmv_matrix A);
+// SELL launch table (the PartArg's rowptr field carries the slice offsets).
+struct SpmvArgs;
+int fill_sell_args(SpmvArgs& a, const DevCsr& C, const int32_t* cols,
+                   const void* vals, size_t es, const void* const* x,
+                   void* const* y, const void* const* xown, int BS, int max_blocks);
 
 void build_halo_tables(spmv_l2gmap map);
 void launch_update(spmv_l2gmap map, spmv_dtype dtype, void* const* vecs,
@@ -282,5 +313,22 @@ double* cg_rhs(spmv_matrix A);
 double* cg_solution(spmv_matrix A);
 void cg_run(spmv_matrix A, int max_its, double rtol, spmv_cg_info* info);
 void destroy_cg_workspace(CgWorkspace* w);
+
+// Mixed-precision CG (ir.cu): same layout as cg_*; the FP32 copy of the
+// values is made on first use.
+void ensure_vals32(spmv_matrix A);
+double* ir_rhs(spmv_matrix A);
+double* ir_solution(spmv_matrix A);
+void ir_run(spmv_matrix A, int max_its, double rtol, spmv_ir_info* info);
+void destroy_ir_workspace(IrWorkspace* w);
+
+// Persistent batched solve (batch.cu) over the concatenated b and x.
+void batch_solve(spmv_batch B, const double* d_b, double* d_x, int max_its,
+                 double rtol, spmv_batch_info* info);
+
+// out[r][k] = scale * lambda[r][row(k)] * x[r][col(k)] (adjoint.cu).
+void launch_sample_outer(spmv_matrix A, double scale, const void* const* lambda,
+                         const void* const* x, void* const* out,
+                         cudaStream_t stream);
 
 }  // namespace spmvb

@@ -136,4 +136,37 @@ __device__ __forceinline__ bool grid_sum(double part, double* partials,
   return true;
 }
 
+// Two sums at once (same scheme as grid_sum; partials holds 2 per CTA).
+template <int BS>
+__device__ __forceinline__ bool grid_sum2(double a, double b, double* partials,
+                                          unsigned int* ticket, double* ta,
+                                          double* tb, double* smem) {
+  __shared__ bool s_last;
+  a = block_sum<BS>(a, smem);
+  b = block_sum<BS>(b, smem);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = a;
+    partials[2 * blockIdx.x + 1] = b;
+    __threadfence();
+    const unsigned int t = atomicAdd(ticket, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  double va = 0.0, vb = 0.0;
+  for (unsigned int i = threadIdx.x; i < gridDim.x; i += BS) {
+    va += __ldcg(partials + 2 * i);
+    vb += __ldcg(partials + 2 * i + 1);
+  }
+  va = block_sum<BS>(va, smem);
+  vb = block_sum<BS>(vb, smem);
+  if (threadIdx.x == 0) {
+    *ta = va;
+    *tb = vb;
+    *ticket = 0u;
+  }
+  return true;
+}
+
 }  // namespace spmvb

@@ -1,0 +1,239 @@
+// SELL-32 (sliced ELLPACK) copy of a matrix, built on the device from its CSR
+// (the product kernel itself is sell_for_rows in spmv_kernel.cuh).
+//
+// Per rank, rows are cut into slices of 32 consecutive rows (no reordering,
+// so y is written in row order); slice s is w_s = max row length in the slice
+// wide and stored column-major: entry k of row 32s+l at soff[s] + 32k + l,
+// padding columns -1 with value 0.  For matrices with even row lengths (the
+// stencils) the padding is about 1%, the row pointers are no longer read, and
+// each lane's loads are independent of each other.
+#include <algorithm>
+
+#include "internal.h"
+#include "spmv_kernel.cuh"
+
+namespace spmvb {
+
+namespace {
+
+inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
+// One thread per (padded) row: copies the row's entries into its SELL
+// column and pads the rest of the slice width.
+template <typename T>
+__global__ void csr_to_sell(const int32_t* __restrict__ rowptr,
+                            const int32_t* __restrict__ cols_in,
+                            const T* __restrict__ vals_in,
+                            const int32_t* __restrict__ soff, int nrows,
+                            int nslices, int32_t* __restrict__ cols_out,
+                            T* __restrict__ vals_out) {
+  const int64_t total = int64_t(nslices) * 32;
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < total;
+       r += int64_t(gridDim.x) * blockDim.x) {
+    const int s = int(r >> 5), l = int(r & 31);
+    const int o = soff[s];
+    const int w = (soff[s + 1] - o) >> 5;
+    const int base = r < nrows ? rowptr[r] : 0;
+    const int len = r < nrows ? rowptr[r + 1] - base : 0;
+    for (int k = 0; k < w; ++k) {
+      const int idx = o + k * 32 + l;
+      if (k < len) {
+        cols_out[idx] = cols_in[base + k];
+        if (vals_out) vals_out[idx] = vals_in[base + k];
+      } else {
+        cols_out[idx] = -1;
+        if (vals_out) vals_out[idx] = T(0);
+      }
+    }
+  }
+}
+
+__global__ void sell_to_float(const double* __restrict__ in, float* __restrict__ out,
+                              int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = float(in[i]);
+}
+
+// Scatters every rank's CSR (cols_in, optional vals_in) into SELL arrays.
+void scatter_all(spmv_matrix A, DevCsr& C, const int32_t* cols_in,
+                 int32_t* cols_out, bool with_vals, cudaStream_t s) {
+  const size_t es = dtype_size(A->dtype);
+  const int grid = std::max(1, A->comm->num_sms) * 8;
+  for (size_t r = 0; r < C.parts.size(); ++r) {
+    const DevPart& D = C.parts[r];
+    const int nslices = (D.nrows + 31) / 32;
+    if (nslices == 0) continue;
+    const int32_t* rp = C.rowptr.as<int32_t>() + D.rp_off;
+    const int32_t* so = C.sell_off.as<int32_t>() + D.sl_off;
+    if (A->dtype == SPMV_FLOAT64) {
+      csr_to_sell<double><<<grid, 256, 0, s>>>(
+          rp, cols_in + D.nz_off, C.vals.as<double>() + D.nz_off, so, D.nrows, nslices,
+          cols_out + D.sz_off, with_vals ? C.sell_vals.as<double>() + D.sz_off : nullptr);
+    } else {
+      csr_to_sell<float><<<grid, 256, 0, s>>>(
+          rp, cols_in + D.nz_off, C.vals.as<float>() + D.nz_off, so, D.nrows, nslices,
+          cols_out + D.sz_off, with_vals ? C.sell_vals.as<float>() + D.sz_off : nullptr);
+    }
+    SPMVB_CUDA(cudaGetLastError());
+  }
+  (void)es;
+}
+
+}  // namespace
+
+// Padded SELL-32 size of a rank's block (host, from its row pointers).
+int64_t sell_padded_size(const std::vector<int32_t>& rowptr, int32_t nrows,
+                         std::vector<int32_t>* soff) {
+  const int nslices = (nrows + 31) / 32;
+  if (soff) soff->assign(size_t(nslices) + 1, 0);
+  int64_t total = 0;
+  for (int s = 0; s < nslices; ++s) {
+    int w = 0;
+    const int r1 = std::min(nrows, (s + 1) * 32);
+    for (int r = s * 32; r < r1; ++r) w = std::max(w, rowptr[r + 1] - rowptr[r]);
+    total += int64_t(w) * 32;
+    if (soff) (*soff)[s + 1] = int32_t(total);
+  }
+  return total;
+}
+
+void build_sell(spmv_matrix A, DevCsr& C, cudaStream_t stream) {
+  if (C.sell_built) return;
+  require(&C == &A->fwd, "spmv: SELL layout is built for the forward matrix only");
+  const int P = A->comm->size;
+  const size_t es = dtype_size(A->dtype);
+  std::vector<int32_t> all_off;
+  int64_t sz = 0;
+  for (int r = 0; r < P; ++r) {
+    DevPart& D = C.parts[r];
+    std::vector<int32_t> soff;
+    const int64_t padded = sell_padded_size(A->h_rowptr[r], D.nrows, &soff);
+    require(padded < (int64_t(1) << 31), "spmv: rank too large for 32-bit SELL offsets");
+    D.sl_off = int64_t(all_off.size());
+    D.sz_off = sz;
+    D.snnz = padded;
+    all_off.insert(all_off.end(), soff.begin(), soff.end());
+    sz = align_up(sz + padded, 32);
+  }
+  C.sl_total = int64_t(all_off.size());
+  C.sz_total = std::max<int64_t>(sz, 32);
+  C.sell_off.reserve(sizeof(int32_t) * std::max<size_t>(all_off.size(), 1));
+  if (!all_off.empty())
+    SPMVB_CUDA(cudaMemcpy(C.sell_off.ptr, all_off.data(), sizeof(int32_t) * all_off.size(),
+                          cudaMemcpyHostToDevice));
+  C.sell_cols.reserve(sizeof(int32_t) * C.sz_total);
+  C.sell_vals.reserve(es * C.sz_total);
+  scatter_all(A, C, C.cols.as<int32_t>(), C.sell_cols.as<int32_t>(), true, stream);
+  SPMVB_CUDA(cudaStreamSynchronize(stream));
+  C.sell_built = true;
+}
+
+void refresh_sell_values(spmv_matrix A) {
+  DevCsr& C = A->fwd;
+  if (!C.sell_built) return;
+  // Same pattern: re-scatter the values (and columns, unchanged) in place.
+  scatter_all(A, C, C.cols.as<int32_t>(), C.sell_cols.as<int32_t>(), true,
+              A->comm->stream);
+  C.sell_vals32.release();
+  SPMVB_CUDA(cudaStreamSynchronize(A->comm->stream));
+}
+
+void build_sell_global(spmv_matrix A) {
+  DevCsr& C = A->fwd;
+  if (C.sell_cols_global.ptr) return;
+  build_global_cols(A);
+  build_sell(A, C, A->comm->stream);
+  C.sell_cols_global.reserve(sizeof(int32_t) * C.sz_total);
+  scatter_all(A, C, C.cols_global.as<int32_t>(), C.sell_cols_global.as<int32_t>(), false,
+              A->comm->stream);
+  SPMVB_CUDA(cudaStreamSynchronize(A->comm->stream));
+}
+
+void build_sell_vals32(spmv_matrix A) {
+  DevCsr& C = A->fwd;
+  if (C.sell_vals32.ptr) return;
+  require(A->dtype == SPMV_FLOAT64, "spmv: FP32 copy needs an FP64 matrix");
+  build_sell(A, C, A->comm->stream);
+  C.sell_vals32.reserve(sizeof(float) * C.sz_total);
+  sell_to_float<<<std::max(1, A->comm->num_sms) * 8, 256, 0, A->comm->stream>>>(
+      C.sell_vals.as<double>(), C.sell_vals32.as<float>(), C.sz_total);
+  SPMVB_CUDA(cudaGetLastError());
+  SPMVB_CUDA(cudaStreamSynchronize(A->comm->stream));
+}
+
+int fill_sell_args(SpmvArgs& a, const DevCsr& C, const int32_t* cols, const void* vals,
+                   size_t es, const void* const* x, void* const* y,
+                   const void* const* xown, int BS, int max_blocks) {
+  a.nparts = int(C.parts.size());
+  const int slices_per_tile = BS / 32;
+  int64_t tiles_total = 0;
+  for (const DevPart& D : C.parts)
+    tiles_total += ((D.nrows + 31) / 32 + slices_per_tile - 1) / slices_per_tile;
+  int blocks = 0;
+  for (int p = 0; p < a.nparts; ++p) {
+    const DevPart& D = C.parts[p];
+    PartArg& P = a.part[p];
+    P.rowptr = C.sell_off.as<int32_t>() + D.sl_off;
+    P.cols = cols + D.sz_off;
+    P.vals = static_cast<const char*>(vals) + D.sz_off * es;
+    P.x = x[p];
+    P.y = y[p];
+    P.xown = xown ? xown[p] : nullptr;
+    P.nrows = D.nrows;
+    P.block_begin = blocks;
+    const int64_t tiles = ((D.nrows + 31) / 32 + slices_per_tile - 1) / slices_per_tile;
+    int64_t nb = tiles;
+    if (tiles_total > max_blocks)
+      nb = std::max<int64_t>(tiles > 0 ? 1 : 0,
+                             (tiles * max_blocks + tiles_total - 1) / tiles_total);
+    P.ntiles = int32_t(tiles);
+    P.nblocks = int32_t(nb);
+    blocks += int(nb);
+  }
+  a.nblocks = blocks;
+  return blocks;
+}
+
+namespace {
+
+template <typename T, int BS>
+void launch_sell_u(const SpmvArgs& a, int U, cudaStream_t s) {
+  switch (U) {
+    case 1: spmv_sell_kernel<T, BS, 1><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 2: spmv_sell_kernel<T, BS, 2><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 4: spmv_sell_kernel<T, BS, 4><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 8: spmv_sell_kernel<T, BS, 8><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 16: spmv_sell_kernel<T, BS, 16><<<a.nblocks, BS, 0, s>>>(a); break;
+    default: fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: SELL width must be 1, 2, 4, 8 or 16");
+  }
+}
+
+}  // namespace
+
+void launch_sell(const SpmvLaunch& L, const int32_t* sell_cols, cudaStream_t stream) {
+  const DevCsr& C = *L.csr;
+  const int U = L.width > 0 ? L.width : 8;
+  const int BS = L.block > 0 ? L.block : 256;
+  const size_t es = dtype_size(L.dtype);
+  SpmvArgs a;
+  fill_sell_args(a, C, sell_cols, C.sell_vals.ptr, es, L.x, L.y, nullptr, BS,
+                 max_blocks_for(L.num_sms, BS));
+  if (a.nblocks == 0) return;
+  if (L.dtype == SPMV_FLOAT64) {
+    switch (BS) {
+      case 128: launch_sell_u<double, 128>(a, U, stream); break;
+      case 256: launch_sell_u<double, 256>(a, U, stream); break;
+      case 512: launch_sell_u<double, 512>(a, U, stream); break;
+    }
+  } else {
+    switch (BS) {
+      case 128: launch_sell_u<float, 128>(a, U, stream); break;
+      case 256: launch_sell_u<float, 256>(a, U, stream); break;
+      case 512: launch_sell_u<float, 512>(a, U, stream); break;
+    }
+  }
+  SPMVB_CUDA(cudaGetLastError());
+}
+
+}  // namespace spmvb

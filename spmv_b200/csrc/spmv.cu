@@ -89,10 +89,16 @@ void launch_vector_bs(const SpmvArgs& a, int W, int BS, cudaStream_t s) {
 
 }  // namespace
 
-spmv_kernel pick_kernel(spmv_kernel requested, const DevCsr& C) {
+spmv_kernel pick_kernel(spmv_kernel requested, const DevCsr& C, bool allow_sell) {
+  if (requested == SPMV_KERNEL_SELL) return allow_sell ? SPMV_KERNEL_SELL : SPMV_KERNEL_VECTOR;
   if (requested != SPMV_KERNEL_AUTO) return requested;
   const double skew_limit = std::max(64.0, 8.0 * C.mean_row);
-  return double(C.max_row) > skew_limit ? SPMV_KERNEL_MERGE : SPMV_KERNEL_VECTOR;
+  if (double(C.max_row) > skew_limit) return SPMV_KERNEL_MERGE;
+  int64_t nnz = 0;
+  for (const DevPart& D : C.parts) nnz += D.nnz;
+  if (allow_sell && nnz > 0 && C.sell_padded > 0 && C.sell_padded <= nnz + nnz / 4)
+    return SPMV_KERNEL_SELL;
+  return SPMV_KERNEL_VECTOR;
 }
 
 int max_blocks_for(int num_sms, int BS) {
@@ -110,9 +116,14 @@ void launch_spmv(const SpmvLaunch& L, cudaStream_t stream) {
           "spmv: width must be 1..32, a power of two");
   require(BS == 128 || BS == 256 || BS == 512,
           "spmv: block must be 128, 256 or 512");
-  if (pick_kernel(L.kernel, *L.csr) == SPMV_KERNEL_MERGE) {
+  const spmv_kernel k = pick_kernel(L.kernel, *L.csr, L.csr->sell_built);
+  if (k == SPMV_KERNEL_MERGE) {
     require(L.carry != nullptr, "spmv: merge-path product needs a carry buffer");
     launch_merge(L, stream, *L.carry);
+    return;
+  }
+  if (k == SPMV_KERNEL_SELL) {
+    launch_sell(L, L.csr->sell_cols.as<int32_t>(), stream);
     return;
   }
   SpmvArgs a;

@@ -64,6 +64,65 @@ __device__ __forceinline__ void for_rows(const SpmvArgs& a, F&& f) {
   }
 }
 
+// SELL-32 (sliced ELLPACK) traversal.  A rank's rows are cut into slices of
+// 32; slice s holds w_s = its longest row's length columns, stored column by
+// column: entry k of row 32s+l is at soff[s] + 32k + l (soff = the
+// PartArg's rowptr field here).  Short rows are padded with column -1.  One
+// warp takes one slice, lane l its row 32s+l, so every load of the warp is a
+// contiguous 256-byte (FP64) or 128-byte run, and each lane issues U value and
+// U column loads before it needs any of them.  A row is summed in storage
+// order (k ascending), the order of the sequential CSR loop.
+template <typename T, int BS, int U, class F>
+__device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f) {
+  const int p = find_part(a, blockIdx.x);
+  const PartArg& P = a.part[p];
+  const int32_t* __restrict__ soff = P.rowptr;
+  const int32_t* __restrict__ cols = P.cols;
+  const T* __restrict__ vals = static_cast<const T*>(P.vals);
+  const T* __restrict__ x = static_cast<const T*>(P.x);
+  const int warp = int(threadIdx.x) >> 5, lane = int(threadIdx.x) & 31;
+  const int nslices = (P.nrows + 31) >> 5;
+  for (int tile = int(blockIdx.x) - P.block_begin; tile < P.ntiles;
+       tile += P.nblocks) {
+    const int slice = tile * (BS / 32) + warp;
+    if (slice >= nslices) continue;  // uniform across the warp
+    const int o = __ldg(soff + slice);
+    const int w = (__ldg(soff + slice + 1) - o) >> 5;
+    T sum = T(0);
+    for (int k0 = 0; k0 < w; k0 += U) {
+      T v[U];
+      int c[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (k0 + u < w) {
+          const int idx = o + (k0 + u) * 32 + lane;
+          v[u] = ld_stream(vals + idx);
+          c[u] = ld_stream(cols + idx);
+        } else {
+          v[u] = T(0);
+          c[u] = -1;
+        }
+      }
+      T xv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) xv[u] = c[u] >= 0 ? ld_gather(x + c[u]) : T(0);
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (c[u] >= 0) sum += v[u] * xv[u];
+    }
+    const int row = slice * 32 + lane;
+    if (row < P.nrows) f(P, row, sum);
+  }
+}
+
+template <typename T, int BS, int U>
+__global__ void __launch_bounds__(BS)
+    spmv_sell_kernel(const __grid_constant__ SpmvArgs a) {
+  sell_for_rows<T, BS, U>(a, [](const PartArg& P, int row, T sum) {
+    static_cast<T*>(P.y)[row] = sum;
+  });
+}
+
 template <typename T, int W, int BS>
 __global__ void __launch_bounds__(BS)
     spmv_vector_kernel(const __grid_constant__ SpmvArgs a) {

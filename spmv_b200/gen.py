@@ -232,3 +232,22 @@ def workload(name: str, scale: int = 0) -> Workload:
         return Workload(name, A, 1, normal(4, 100, A.nrows), 1e-10,
                         {"xstar": normal(4, 101, A.nrows)})
     raise ValueError(name)
+
+
+def c4_sizes(count: int = 256, lo: int = 4096, hi: int = 131072, seed: int = 3):
+    """System sizes of the batched workload: integers uniform in [lo, hi]."""
+    u = uniform(seed, 200, count, 0.0, 1.0)
+    return [int(lo + int(v * (hi - lo + 1))) for v in u]
+
+
+def c4_systems(count: int = 256, lo: int = 4096, hi: int = 131072, seed: int = 3,
+               k: int = 12, shift: float = 1e-2):
+    """The batched workload: `count` k-NN graph Laplacians over uniform points
+    in the unit cube (w = exp(-d^2/h^2), h = mean k-NN distance per system,
+    +shift on the diagonal), with b ~ N(0,1) per system (stream 300 + i).
+    Returns a list of (CSR, b)."""
+    out = []
+    for i, n in enumerate(c4_sizes(count, lo, hi, seed)):
+        A = knn_laplacian(n, k, seed, i, shift)
+        out.append((A, normal(seed, 300 + i, n)))
+    return out

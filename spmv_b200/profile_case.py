@@ -1,0 +1,55 @@
+"""Runs the kernels of one workload a few times, for profilers (ncu).
+
+    python -m spmv_b200.profile_case --case c2 --reps 3 [--what matvec|cg]
+
+`matvec` runs the reference matvec demo's loop body (matvecmain.cpp:70-86):
+L2GMap::update then Matrix::mult over all ranks, `reps` times, as plain
+kernel launches.  `cg` runs one spmv::cg solve (a CUDA graph).
+"""
+from __future__ import annotations
+
+import argparse
+
+import numpy as np
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="c2")
+    ap.add_argument("--scale", type=int, default=0)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--what", default="matvec", choices=["matvec", "cg"])
+    ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "vector", "merge", "sell"])
+    args = ap.parse_args()
+
+    import torch
+    import spmv_b200 as S
+    from spmv_b200 import gen
+
+    W = gen.workload(args.case, args.scale)
+    D = gen.distribute(W.A, W.P)
+    dt = np.float64 if args.dtype == "f64" else np.float32
+    tdt = torch.float64 if args.dtype == "f64" else torch.float32
+    comm = S.Comm(size=W.P, device=0)
+    cm = S.L2GMap(comm, D.local_sizes, D.ghosts)
+    rm = S.L2GMap(comm, D.local_sizes, [[] for _ in range(W.P)])
+    M = S.Matrix(comm, [(rp, ci, va.astype(dt)) for rp, ci, va in D.blocks], cm, rm)
+    M.set_kernel(args.kernel)
+    if args.what == "matvec":
+        xs = [torch.rand(cm.vec_len(q), dtype=tdt, device="cuda") for q in range(W.P)]
+        ys = [torch.empty(D.local_sizes[q], dtype=tdt, device="cuda") for q in range(W.P)]
+        for _ in range(args.reps):
+            cm.update(xs)
+            M.mult(xs, out=ys)
+        comm.synchronize()
+        print("matvec", args.case, "reps", args.reps, "kernel", M.get_kernel())
+    else:
+        b = [torch.from_numpy(W.b[D.ranges[q]:D.ranges[q + 1]].copy()).cuda()
+             for q in range(W.P)]
+        x, k = S.cg(comm, M, b, 10000, W.rtol)
+        print("cg", args.case, "iterations", k)
+
+
+if __name__ == "__main__":
+    main()

@@ -176,3 +176,60 @@ def test_auto_picks_merge_for_a_dense_row(cuda_device):
     yref = oracle.csr_mult(rp, cols.astype(np.int32), D.blocks[0][2].astype(np.float32),
                            xs[0].astype(np.float32))
     assert_spmv_close(y32, yref, abs_mult(D.blocks[0], xs[0]).astype(np.float32), TOL_F32)
+
+
+@pytest.mark.parametrize("cfg,P", [("c1", 1), ("c2", 8), ("c3", 1)])
+def test_sell_is_bitwise_equal_to_oracle(cuda_device, cfg, P):
+    # SELL-32 sums each row in storage order, like the reference's row loop.
+    W = gen.workload(cfg, scale=0 if cfg != "c3" else 40)
+    comm, cm, rm, M, D = build(W, P)
+    assert M.get_kernel()[0] == "sell"  # chosen automatically for stencils
+    rng = np.random.default_rng(4)
+    xs = [rng.uniform(-1, 1, cm.vec_len(q)) for q in range(P)]
+    ys = M.mult(xs)
+    for q in range(P):
+        rp, ci, va = D.blocks[q]
+        assert np.array_equal(ys[q], oracle.csr_mult(rp, ci, va, xs[q]))
+    M32 = S.Matrix(comm, [(rp, ci, va.astype(np.float32)) for rp, ci, va in D.blocks],
+                   cm, rm)
+    ys32 = M32.mult([x.astype(np.float32) for x in xs])
+    for q in range(P):
+        rp, ci, va = D.blocks[q]
+        assert np.array_equal(ys32[q], oracle.csr_mult(rp, ci, va.astype(np.float32),
+                                                       xs[q].astype(np.float32)))
+
+
+@pytest.mark.parametrize("width", [1, 2, 4, 8, 16])
+@pytest.mark.parametrize("block", [128, 256, 512])
+def test_sell_every_width_and_block(cuda_device, width, block):
+    rng = np.random.default_rng(width * 7 + block)
+    A = random_csr(rng, 2999, 2999, density=0.004, long_rows=(7, 2500))
+    comm, cm, rm, M, D = build(A, 3)
+    M.set_kernel("sell", width, block)
+    assert M.get_kernel() == ("sell", width, block)
+    xs = [rng.standard_normal(cm.vec_len(q)) for q in range(3)]
+    ys = M.mult(xs)
+    for q in range(3):
+        rp, ci, va = D.blocks[q]
+        assert np.array_equal(ys[q], oracle.csr_mult(rp, ci, va, xs[q]))
+
+
+def test_set_values_reaches_every_kernel_copy(cuda_device):
+    # New values must reach the SELL copy and the solvers' graphs, not only
+    # the CSR (one matrix re-used with changing values, as in a parameter
+    # sweep or finite differences).
+    W = gen.workload("c1", scale=48)
+    comm, cm, rm, M, D = build(W, 1)
+    assert M.get_kernel()[0] == "sell"
+    b = [W.b.copy()]
+    x1, k1 = S.cg(comm, M, b, 10000, 1e-10)
+    xm1, _ = S.cg_mixed(comm, M, b, 10000, 1e-10)
+    M.set_values([D.blocks[0][2] * 4.0])
+    xs = [np.random.default_rng(0).standard_normal(cm.vec_len(0))]
+    y = M.mult(xs)[0]
+    rp, ci, va = D.blocks[0]
+    assert np.array_equal(y, oracle.csr_mult(rp, ci, va * 4.0, xs[0]))
+    x2, k2 = S.cg(comm, M, b, 10000, 1e-10)
+    xm2, _ = S.cg_mixed(comm, M, b, 10000, 1e-10)
+    assert np.allclose(x2[0] * 4.0, x1[0], rtol=1e-7, atol=1e-12)
+    assert np.allclose(xm2[0] * 4.0, xm1[0], rtol=1e-7, atol=1e-12)

@@ -31,6 +31,7 @@ def check_against_mult(M, D, xs_host, tol):
     for _ in range(2):
         ys = [torch.full((n,), float("nan"), dtype=xs[0].dtype, device="cuda")
               for n in M.nrows]
+        torch.cuda.synchronize()  # the fill runs on torch's stream
         noalloc(M, xs, ys)
         torch.cuda.synchronize()
         for q in range(D.P):
