@@ -131,6 +131,7 @@ def setup(device: int):
     cm = S.L2GMap(comm, D.local_sizes, D.ghosts)
     rm = S.L2GMap(comm, D.local_sizes, [[] for _ in range(W.P)])
     M = S.Matrix(comm, D.blocks, cm, rm)
+    M.autotune(reps=10)  # the plan step: pick kernel, width and block
     return W, D, comm, cm, rm, M
 
 
@@ -194,6 +195,133 @@ def config_dict(W, D, P, extra=None):
     if extra:
         c.update(extra)
     return c
+
+
+# ---------------------------------------------------------------------------
+# Mixed-precision and batched solves against plain FP64 GPU CG (rel-res 1e-10)
+# ---------------------------------------------------------------------------
+def _timed(stream, fn, reps):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps, out
+
+
+def run_extras(device: int, reps: int, c4_count: int):
+    """c3: 27-point lognormal Laplacian 160^3 (4,096,000 rows), FP64 CG vs
+    mixed CG, both to ||b - A x|| / ||b|| < 1e-10.  c4: `c4_count` k-NN
+    systems of 4,096..131,072 rows, one batched persistent launch vs one
+    plain FP64 CG solve per system.  c5: one adjoint (forward solve, adjoint
+    solve, dL/dA sampling) on the 1024^2 grid."""
+    import torch
+    import spmv_b200 as S
+    from spmv_b200 import gen
+    from spmv_b200.core import Batch
+    out = {}
+    # c3 ----------------------------------------------------------------------
+    t0 = time.perf_counter()
+    W = gen.workload("c3")
+    comm = S.Comm(size=1, device=device)
+    stream = comm.torch_stream()
+    cm = S.L2GMap(comm, [W.A.nrows], [[]])
+    M = S.Matrix(comm, [(W.A.rowptr, W.A.cols, W.A.vals)], cm, cm)
+    tune = M.autotune(reps=5)
+    b = [torch.from_numpy(W.b).cuda(device)]
+    x64 = [torch.zeros_like(b[0])]
+    xm = [torch.zeros_like(b[0])]
+    _, k64 = S.cg(comm, M, b, 20000, 1e-10, x=x64)
+    _, im = S.cg_mixed(comm, M, b, 20000, 1e-10, x=xm)
+    setup_s = time.perf_counter() - t0
+    t64, (_, k64) = _timed(stream, lambda: S.cg(comm, M, b, 20000, 1e-10, x=x64), reps)
+    tmx, (_, im) = _timed(stream, lambda: S.cg_mixed(comm, M, b, 20000, 1e-10, x=xm), reps)
+    r = M.mult(xm)[0]
+    relres_m = float(torch.linalg.norm(b[0] - r) / torch.linalg.norm(b[0]))
+    r = M.mult(x64)[0]
+    relres_64 = float(torch.linalg.norm(b[0] - r) / torch.linalg.norm(b[0]))
+    err = float(torch.linalg.norm(xm[0] - x64[0]) / torch.linalg.norm(x64[0]))
+    out["c3_mixed_vs_fp64"] = {
+        "fp64_cg_solves_per_s": 1.0 / t64, "fp64_iterations": k64,
+        "mixed_solves_per_s": 1.0 / tmx, "mixed_inner_iterations": im.iterations,
+        "mixed_refinements": im.refinements, "speedup": t64 / tmx,
+        "relres_fp64": relres_64, "relres_mixed": relres_m,
+        "error_mixed_vs_fp64_solution": err, "kernel": tune[:3],
+        "setup_s": setup_s}
+    del M, cm, b, x64, xm
+    torch.cuda.empty_cache()
+    # c4 ----------------------------------------------------------------------
+    t0 = time.perf_counter()
+    systems = gen.c4_systems(count=c4_count)
+    gen_s = time.perf_counter() - t0
+    comm4 = S.Comm(size=1, device=device)
+    stream4 = comm4.torch_stream()
+    B = Batch(comm4, [(A.rowptr, A.cols, A.vals) for A, _ in systems])
+    bb = [torch.from_numpy(bv).cuda(device) for _, bv in systems]
+    xb = [torch.zeros_like(v) for v in bb]
+    best = None
+    for cl in (1, 2, 4, 8):      # cluster size, picked by timing
+        B.set_cluster(cl)
+        tb, (_, info) = _timed(stream4, lambda: B.solve(bb, 20000, 1e-10, x=xb), 1)
+        if best is None or tb < best[1]:
+            best = (cl, tb)
+    B.set_cluster(best[0])
+    tb, (_, info) = _timed(stream4, lambda: B.solve(bb, 20000, 1e-10, x=xb), reps)
+    conv = sum(int(i.converged) for i in info)
+    worst = max(i.relres for i in info)
+    mats = []
+    for A, _ in systems:
+        c1 = S.L2GMap(comm4, [A.nrows], [[]])
+        mats.append((c1, S.Matrix(comm4, [(A.rowptr, A.cols, A.vals)], c1, c1)))
+    x1 = [torch.zeros_like(v) for v in bb]
+
+    def plain():
+        its = 0
+        for (c1, Mi), bi, xi in zip(mats, bb, x1):
+            _, k = S.cg(comm4, Mi, [bi], 20000, 1e-10, x=[xi])
+            its += k
+        return its
+
+    plain()  # builds the per-system graphs
+    tp, its64 = _timed(stream4, plain, 1)
+    n_rows = sum(A.nrows for A, _ in systems)
+    n_nnz = sum(A.nnz for A, _ in systems)
+    out["c4_batched_vs_fp64"] = {
+        "systems": len(systems), "rows": n_rows, "nnz": n_nnz,
+        "batched_batches_per_s": 1.0 / tb,
+        "batched_system_solves_per_s": len(systems) / tb,
+        "fp64_per_system_system_solves_per_s": len(systems) / tp,
+        "speedup": tp / tb, "cluster": best[0], "converged": conv,
+        "worst_relres": worst, "inner_iterations_total": sum(i.iterations for i in info),
+        "fp64_iterations_total": its64,
+        "h_mean": float(np.mean([A.scalar for A, _ in systems])),
+        "generation_s": gen_s}
+    del mats, B
+    torch.cuda.empty_cache()
+    # c5 ----------------------------------------------------------------------
+    from spmv_b200.autograd import SpdSystem, spd_solve
+    G = gen.grid2d_softplus(1024, 1024, 4, 0.5, 1e-3)
+    sysm = SpdSystem(G.rowptr, G.cols, G.vals, device=device, rtol=1e-12)
+    bt = torch.from_numpy(gen.normal(4, 100, G.nrows)).cuda(device)
+    xs = torch.from_numpy(gen.normal(4, 101, G.nrows)).cuda(device)
+    vals = torch.from_numpy(G.vals).cuda(device).requires_grad_(True)
+
+    def adjoint():
+        vals.grad = None
+        x = spd_solve(vals, bt, sysm)
+        L = 0.5 * ((x - xs) ** 2).sum()
+        L.backward()
+        return L
+
+    adjoint()
+    ta, _ = _timed(torch.cuda.current_stream(device), adjoint, 1)
+    out["c5_adjoint"] = {"forward_plus_adjoint_s": ta,
+                         "cg_iterations": sysm.last_iterations[-2:],
+                         "edges": int(2 * 1024 * 1023)}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -346,6 +474,10 @@ def run_ours(args, world, rank, local):
                          "iterations timed (%.1f s), scaled to the %.0f iterations "
                          "of a full solve" % (nth, kk, spi * kk, k_mean)}
 
+    extras = None
+    if world == 1 and not args.no_extras:
+        extras = run_extras(device, args.extra_reps, args.c4_count)
+
     if rank == 0:
         line = {
             "metric": "CG solves/s", "value": value, "unit": "solves/s",
@@ -374,6 +506,8 @@ def run_ours(args, world, rank, local):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if extras:
+            line["extras"] = extras
         print(json.dumps(line), flush=True)
 
 
@@ -387,6 +521,10 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--ref-budget", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the c3/c4/c5 mixed, batched and adjoint measurements")
+    ap.add_argument("--extra-reps", type=int, default=2)
+    ap.add_argument("--c4-count", type=int, default=256)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

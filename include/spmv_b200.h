@@ -227,6 +227,22 @@ int spmv_matrix_set_kernel(spmv_matrix A, spmv_kernel kernel, int width,
 int spmv_matrix_get_kernel(spmv_matrix A, spmv_kernel* kernel, int* width,
                            int* block);
 
+typedef struct spmv_tune_result {
+  spmv_kernel kernel;  /* chosen kernel family                               */
+  int width;           /* lanes per row (vector) or loads per lane (SELL)    */
+  int block;           /* threads per CTA                                    */
+  double us;           /* time of one product with that choice, microseconds */
+  int candidates;      /* configurations timed (0: taken from the cache)     */
+} spmv_tune_result;
+
+/* Autotuner (no counterpart in the reference; mkl_sparse_optimize,
+ * Matrix.cpp:43, is the reference's analysis step): times the product over
+ * candidate kernels, widths and block sizes on this matrix, `reps` launches
+ * each, and keeps the fastest for mult and for the solvers.  Allocates scratch
+ * vectors for the timing.  With the environment variable SPMV_B200_TUNE_CACHE
+ * naming a file, results are cached there by matrix statistics. */
+int spmv_matrix_autotune(spmv_matrix A, int reps, spmv_tune_result* best);
+
 /* ------------------------------------------------------------------------ */
 /* Conjugate gradients (reference: cg.h:27-29, cg.cpp:11-83)                 */
 /* ------------------------------------------------------------------------ */
@@ -276,6 +292,23 @@ typedef struct spmv_ir_info {
 int spmv_cg_mixed(spmv_matrix A, spmv_memory memory, const double* const* b,
                   const int64_t* b_rows, double* const* x, int max_its,
                   double rtol, spmv_ir_info* info);
+
+/* ------------------------------------------------------------------------ */
+/* Several right-hand sides (no counterpart in the reference)                */
+/* ------------------------------------------------------------------------ */
+
+/* Y[r] = A[r] X[r] for nrhs (1..32) right-hand sides at once, reading A once:
+ * X[r] is ncols[r] x nrhs and Y[r] nrows[r] x nrhs, row-major (the nrhs values
+ * of one row contiguous). */
+int spmv_matrix_mult_block(spmv_matrix A, int nrhs, spmv_memory memory,
+                           const void* const* x, void* const* y);
+/* Block CG: nrhs (1..32) independent CG solves (the recurrence of spmv::cg,
+ * cg.cpp:11-83, per column, each with its own stopping test) sharing one
+ * product per iteration.  b[r] is local_size x nrhs, x[r] (local_size +
+ * num_ghosts) x nrhs (ghost rows zero), row-major; info[nrhs] may be NULL. */
+int spmv_cg_block(spmv_matrix A, int nrhs, spmv_memory memory,
+                  const double* const* b, double* const* x, int max_its,
+                  double rtol, spmv_cg_info* info);
 
 /* ------------------------------------------------------------------------ */
 /* Batched solves (no counterpart in the reference; builds on spmv::cg)      */

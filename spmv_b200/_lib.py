@@ -52,6 +52,11 @@ class IrInfo(C.Structure):
 BatchInfo = IrInfo  # same layout as spmv_batch_info
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("kernel", C.c_int), ("width", C.c_int), ("block", C.c_int),
+                ("us", C.c_double), ("candidates", C.c_int)]
+
+
 _p = C.c_void_p
 _i32 = C.c_int32
 _i64 = C.c_int64
@@ -108,6 +113,9 @@ _SIGS = {
     "spmv_batch_destroy": [_p],
     "spmv_batch_set_cluster": [_p, _int],
     "spmv_batch_solve": [_p, _int, _pp, _pp, _int, C.c_double, C.POINTER(IrInfo)],
+    "spmv_matrix_autotune": [_p, _int, C.POINTER(TuneResult)],
+    "spmv_matrix_mult_block": [_p, _int, _int, _pp, _pp],
+    "spmv_cg_block": [_p, _int, _int, _pp, _pp, _int, C.c_double, C.POINTER(CgInfo)],
 }
 
 _lib = None

@@ -33,7 +33,7 @@ CXX = "g++"  # the system compiler (has OpenMP)
 LIB = PKG / "libspmv_b200.so"
 GEN = PKG / "libspmv_gen.so"
 
-CUDA_SOURCES = ["api.cpp", "l2gmap.cpp", "spmv.cu", "merge.cu", "halo.cu", "cg.cu", "ir.cu", "adjoint.cu", "sell.cu", "batch.cu"]
+CUDA_SOURCES = ["api.cpp", "l2gmap.cpp", "spmv.cu", "merge.cu", "halo.cu", "cg.cu", "ir.cu", "adjoint.cu", "sell.cu", "batch.cu", "tune.cpp", "block.cu"]
 HEADERS = ["internal.h", "kernels.cuh", "spmv_kernel.cuh"]
 
 
@@ -70,15 +70,19 @@ def build_lib(force: bool = False, verbose: bool = False) -> Path:
             if verbose:
                 print(r.stdout + r.stderr)
     if force or jobs or _newer(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", str(LIB)] + [str(o) for o in objs])
+        tmp = LIB.with_suffix(".so.tmp")
+        _run([NVCC] + ARCH + ["-shared", "-o", str(tmp)] + [str(o) for o in objs])
+        os.replace(tmp, LIB)  # readers never see a half-written library
     return LIB
 
 
 def build_gen(force: bool = False) -> Path:
     src = CSRC / "gen.cpp"
     if force or _newer(GEN, [src, CSRC / "spmv_gen.h"]):
+        tmp = GEN.with_suffix(".so.tmp")
         _run([CXX, "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared",
-              "-I" + str(CSRC), str(src), "-o", str(GEN)])
+              "-I" + str(CSRC), str(src), "-o", str(tmp)])
+        os.replace(tmp, GEN)
     return GEN
 
 

@@ -307,6 +307,31 @@ class Matrix:
              "merge": _lib.KERNEL_MERGE, "sell": _lib.KERNEL_SELL}[kernel]
         call("spmv_matrix_set_kernel", self._h, k, width, block)
 
+    def mult_block(self, X: Sequence, out: Optional[List] = None) -> List:
+        """Y[r] = A[r] X[r] for X[r] of shape (ncols[r], k), k <= 32, row-major."""
+        mem, dt, ptrs = _vec_info(X)
+        k = int(X[0].shape[1])
+        if out is None:
+            if _is_torch(X[0]):
+                import torch
+                out = [torch.empty((n, k), dtype=X[0].dtype, device=X[0].device)
+                       for n in self.nrows]
+            else:
+                out = [np.empty((n, k), dtype=X[0].dtype) for n in self.nrows]
+        _, _, optrs = _vec_info(out)
+        with self.comm.fence(X):
+            call("spmv_matrix_mult_block", self._h, k, mem, ptr_array(ptrs),
+                 ptr_array(optrs))
+        return out
+
+    def autotune(self, reps: int = 10):
+        """Times the candidate kernels on this matrix and keeps the fastest;
+        returns (kernel, width, block, microseconds, candidates timed)."""
+        r = _lib.TuneResult()
+        call("spmv_matrix_autotune", self._h, int(reps), C.byref(r))
+        names = {0: "auto", 1: "vector", 2: "merge", 3: "sell"}
+        return names[r.kernel], r.width, r.block, r.us, r.candidates
+
     def get_kernel(self):
         k, w, b = C.c_int(), C.c_int(), C.c_int()
         call("spmv_matrix_get_kernel", self._h, C.byref(k), C.byref(w), C.byref(b))
@@ -409,6 +434,28 @@ def cg_mixed(comm: Comm, A: Matrix, b: Sequence, max_its: int, rtol: float,
                                       C.byref(info))
     _lib.check(st)
     return x, info
+
+
+def cg_block(comm: Comm, A: Matrix, B: Sequence, max_its: int, rtol: float,
+             X: Optional[List] = None):
+    """Block CG: k independent solves (B[r] of shape (local_size, k)) sharing
+    one SpMM per iteration.  Returns (X, [CgInfo] * k)."""
+    mem, dt, bptrs = _vec_info(B)
+    k = int(B[0].shape[1])
+    cm = A.col_map()
+    if X is None:
+        lens = [cm.vec_len(r) for r in range(comm.size)]
+        if _is_torch(B[0]):
+            import torch
+            X = [torch.empty((n, k), dtype=B[0].dtype, device=B[0].device) for n in lens]
+        else:
+            X = [np.empty((n, k), dtype=B[0].dtype) for n in lens]
+    _, _, xptrs = _vec_info(X)
+    info = (_lib.CgInfo * k)()
+    with comm.fence(B):
+        call("spmv_cg_block", A.handle, k, mem, ptr_array(bptrs), ptr_array(xptrs),
+             int(max_its), float(rtol), info)
+    return X, list(info)
 
 
 class Batch:

@@ -342,10 +342,9 @@ void halo(spmv_l2gmap map, bool reverse, spmv_dtype dtype, spmv_memory memory,
 }  // namespace spmvb
 
 namespace spmvb {
-namespace {
 
-// Checks shared by spmv_cg and spmv_cg_mixed (cg.cpp:22-28 and the layout
-// the fused-halo solve needs).
+// Checks shared by the solvers (cg.cpp:22-28 and the layout the fused-halo
+// solve needs).
 void check_solve_args(spmv_matrix A, spmv_memory memory, const double* const* b,
                       const int64_t* b_rows, double* const* x) {
   check_mat(A);
@@ -408,7 +407,6 @@ void copy_solution_out(spmv_matrix A, spmv_memory memory, const double* dx,
   SPMVB_CUDA(cudaStreamSynchronize(s));
 }
 
-}  // namespace
 }  // namespace spmvb
 
 using namespace spmvb;
@@ -874,7 +872,9 @@ int spmv_matrix_get_kernel(spmv_matrix A, spmv_kernel* kernel, int* width,
     check_mat(A);
     require(kernel && width && block, "spmv: NULL output");
     *kernel = pick_kernel(A->kernel, A->fwd);
-    if (A->width > 0)
+    if (*kernel == SPMV_KERNEL_MERGE)
+      *width = 0;  // merge-path tiles do not depend on a width
+    else if (A->width > 0)
       *width = A->width;
     else
       *width = *kernel == SPMV_KERNEL_SELL ? 8 : auto_width(A->fwd.mean_row, A->dtype);

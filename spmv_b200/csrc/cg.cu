@@ -68,13 +68,14 @@ struct CgPtrs {
 __global__ void __launch_bounds__(EW_BS)
     cg_init(const CgPtrs c, cudaGraphConditionalHandle h) {
   __shared__ double smem[32];
+  const uint64_t keep = l2_policy_keep();
   double acc = 0.0;
   for (int64_t i = blockIdx.x * int64_t(EW_BS) + threadIdx.x; i < c.n;
        i += int64_t(gridDim.x) * EW_BS) {
     const double bi = c.b[i];
-    c.r[i] = bi;
-    c.p[i] = bi;
-    c.x[i] = 0.0;
+    st_pol(c.r + i, bi, keep);
+    st_pol(c.p + i, bi, keep);
+    st_pol(c.x + i, 0.0, keep);
     acc += bi * bi;
   }
   const double part = block_sum<EW_BS>(acc, smem);
@@ -115,10 +116,11 @@ __global__ void __launch_bounds__(BS)
                      cudaGraphConditionalHandle h) {
   __shared__ double smem[32];
   if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
+  const uint64_t keep = l2_policy_keep();
   double acc = 0.0;
-  sell_for_rows<double, BS, U>(a, [&](const PartArg& P, int row, double sum) {
-    static_cast<double*>(P.y)[row] = sum;
-    acc += static_cast<const double*>(P.xown)[row] * sum;
+  sell_for_rows<double, BS, U, true>(a, [&](const PartArg& P, int row, double sum) {
+    st_pol(static_cast<double*>(P.y) + row, sum, keep);
+    acc += ld_pol(static_cast<const double*>(P.xown) + row, keep) * sum;
   });
   cg_dot_finish<BS>(acc, c, smem);
 }
@@ -152,13 +154,14 @@ __global__ void __launch_bounds__(EW_BS)
   __shared__ double smem[32];
   const bool ok = c.st->status == SPMV_SUCCESS;
   const double alpha = c.st->alpha;
+  const uint64_t keep = l2_policy_keep();
   double acc = 0.0;
   if (ok) {
     for (int64_t i = blockIdx.x * int64_t(EW_BS) + threadIdx.x; i < c.n;
          i += int64_t(gridDim.x) * EW_BS) {
-      c.x[i] = c.x[i] + alpha * c.p[i];
-      const double ri = c.r[i] - alpha * c.y[i];
-      c.r[i] = ri;
+      st_pol(c.x + i, ld_pol(c.x + i, keep) + alpha * ld_pol(c.p + i, keep), keep);
+      const double ri = ld_pol(c.r + i, keep) - alpha * ld_pol(c.y + i, keep);
+      st_pol(c.r + i, ri, keep);
       acc += ri * ri;
     }
   }
@@ -183,9 +186,10 @@ __global__ void __launch_bounds__(EW_BS)
 __global__ void __launch_bounds__(EW_BS) cg_update_p(const CgPtrs c) {
   if (c.st->status != SPMV_SUCCESS) return;
   const double beta = c.st->beta;
+  const uint64_t keep = l2_policy_keep();
   for (int64_t i = blockIdx.x * int64_t(EW_BS) + threadIdx.x; i < c.n;
        i += int64_t(gridDim.x) * EW_BS)
-    c.p[i] = c.p[i] * beta + c.r[i];
+    st_pol(c.p + i, ld_pol(c.p + i, keep) * beta + ld_pol(c.r + i, keep), keep);
 }
 
 using DotFn = void (*)(SpmvArgs, CgPtrs, cudaGraphConditionalHandle);

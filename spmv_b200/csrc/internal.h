@@ -322,6 +322,20 @@ double* ir_solution(spmv_matrix A);
 void ir_run(spmv_matrix A, int max_its, double rtol, spmv_ir_info* info);
 void destroy_ir_workspace(IrWorkspace* w);
 
+// Solver argument checks and global-layout copies (api.cpp).
+void check_solve_args(spmv_matrix A, spmv_memory memory, const double* const* b,
+                      const int64_t* b_rows, double* const* x);
+void copy_rhs_in(spmv_matrix A, spmv_memory memory, const double* const* b, double* db);
+void copy_solution_out(spmv_matrix A, spmv_memory memory, const double* dx,
+                       double* const* x);
+
+// Multi-right-hand-side product and block CG (block.cu); blocks are row-major
+// with leading dimension k.
+void launch_spmm(spmv_matrix A, int k, const void* const* x, void* const* y,
+                 cudaStream_t stream);
+void block_cg(spmv_matrix A, int k, const double* d_b, double* d_x, int max_its,
+              double rtol, spmv_cg_info* info);
+
 // Persistent batched solve (batch.cu) over the concatenated b and x.
 void batch_solve(spmv_batch B, const double* d_b, double* d_x, int max_its,
                  double rtol, spmv_batch_info* info);

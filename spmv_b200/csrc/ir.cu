@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(EW) ir_init(const IrPtrs c, cudaGraphCondition
 template <typename T, int W, bool SELL, class F>
 __device__ __forceinline__ void rows_of(const SpmvArgs& a, F&& f) {
   if constexpr (SELL)
-    sell_for_rows<T, 256, W>(a, f);
+    sell_for_rows<T, 256, W, true>(a, f);  // vectors kept in L2, matrix streamed
   else
     for_rows<T, W, 256>(a, f);
 }
@@ -123,9 +123,10 @@ __global__ void __launch_bounds__(256)
   __shared__ double smem[32];
   if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h_loop, 0u);
   double acc = 0.0;
+  const uint64_t keep = l2_policy_keep();
   rows_of<float, W, SELL>(a, [&](const PartArg& P, int row, float sum) {
-    static_cast<float*>(P.y)[row] = sum;
-    acc += double(static_cast<const float*>(P.xown)[row]) * double(sum);
+    st_pol(static_cast<float*>(P.y) + row, sum, keep);
+    acc += double(ld_pol(static_cast<const float*>(P.xown) + row, keep)) * double(sum);
   });
   const double part = block_sum<256>(acc, smem);
   double total;
@@ -143,12 +144,13 @@ __global__ void __launch_bounds__(EW)
   __shared__ double smem[32];
   const bool ok = c.st->status == SPMV_SUCCESS;
   const float alpha = float(c.st->alpha);
+  const uint64_t keep = l2_policy_keep();
   double acc = 0.0;
   if (ok) {
     IR_LOOP(i) {
-      c.d[i] = c.d[i] + alpha * c.p[i];
-      const float ri = c.r[i] - alpha * c.y[i];
-      c.r[i] = ri;
+      st_pol(c.d + i, ld_pol(c.d + i, keep) + alpha * ld_pol(c.p + i, keep), keep);
+      const float ri = ld_pol(c.r + i, keep) - alpha * ld_pol(c.y + i, keep);
+      st_pol(c.r + i, ri, keep);
       acc += double(ri) * double(ri);
     }
   }
@@ -235,9 +237,10 @@ __global__ void __launch_bounds__(EW)
   if (!stop) {
     const float beta = float(st->beta);
     const float cc = float(st->c);
+    const uint64_t keep = l2_policy_keep();
     IR_LOOP(i) {
-      const float ri = c.r[i];
-      c.p[i] = ri + beta * (c.p[i] - cc * ri);
+      const float ri = ld_pol(c.r + i, keep);
+      st_pol(c.p + i, ri + beta * (ld_pol(c.p + i, keep) - cc * ri), keep);
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {

@@ -75,6 +75,45 @@ __device__ __forceinline__ T ld_gather(const T* p) {
   return __ldg(p);
 }
 
+// L2 cache policies (per-instruction hints; no device setting is touched).
+// Solver vectors are re-read every iteration and fit in L2 with room to
+// spare, the matrix is streamed once per iteration: vector accesses carry an
+// evict-last policy, matrix loads an evict-first one, so the matrix stream
+// does not push the vectors out.
+__device__ __forceinline__ uint64_t l2_policy_keep() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_stream() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ double ld_pol(const double* a, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_pol(const float* a, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int ld_pol(const int* a, uint64_t pol) {
+  int v;
+  asm volatile("ld.global.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_pol(double* a, double v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void st_pol(float* a, float v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol)
+               : "memory");
+}
+
 // Rank owning CTA `b` of a launch (ranks' CTA ranges are ascending).
 __device__ __forceinline__ int find_part(const SpmvArgs& a, int b) {
   int lo = 0, hi = a.nparts - 1;

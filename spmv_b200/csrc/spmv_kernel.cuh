@@ -72,8 +72,17 @@ __device__ __forceinline__ void for_rows(const SpmvArgs& a, F&& f) {
 // contiguous 256-byte (FP64) or 128-byte run, and each lane issues U value and
 // U column loads before it needs any of them.  A row is summed in storage
 // order (k ascending), the order of the sequential CSR loop.
-template <typename T, int BS, int U, class F>
+//
+// KEEP (the solvers): matrix loads carry an L2 evict-first policy and the
+// x gathers an evict-last one, so vectors re-read every iteration stay in L2
+// while the matrix streams through it.
+template <typename T, int BS, int U, bool KEEP = false, class F>
 __device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f) {
+  uint64_t keep = 0, stream = 0;
+  if (KEEP) {
+    keep = l2_policy_keep();
+    stream = l2_policy_stream();
+  }
   const int p = find_part(a, blockIdx.x);
   const PartArg& P = a.part[p];
   const int32_t* __restrict__ soff = P.rowptr;
@@ -96,8 +105,13 @@ __device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f) {
       for (int u = 0; u < U; ++u) {
         if (k0 + u < w) {
           const int idx = o + (k0 + u) * 32 + lane;
-          v[u] = ld_stream(vals + idx);
-          c[u] = ld_stream(cols + idx);
+          if (KEEP) {
+            v[u] = ld_pol(vals + idx, stream);
+            c[u] = ld_pol(cols + idx, stream);
+          } else {
+            v[u] = ld_stream(vals + idx);
+            c[u] = ld_stream(cols + idx);
+          }
         } else {
           v[u] = T(0);
           c[u] = -1;
@@ -105,7 +119,12 @@ __device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f) {
       }
       T xv[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) xv[u] = c[u] >= 0 ? ld_gather(x + c[u]) : T(0);
+      for (int u = 0; u < U; ++u) {
+        if (KEEP)
+          xv[u] = c[u] >= 0 ? ld_pol(x + c[u], keep) : T(0);
+        else
+          xv[u] = c[u] >= 0 ? ld_gather(x + c[u]) : T(0);
+      }
 #pragma unroll
       for (int u = 0; u < U; ++u)
         if (c[u] >= 0) sum += v[u] * xv[u];
