@@ -136,34 +136,19 @@ def setup(device: int):
 
 
 def dist_init():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=None)
-    return world, rank, local
+    from spmv_b200 import ranks
+    info = ranks.init("nccl")
+    return info
 
 
-def max_over_ranks(v: float, world: int, device: int) -> float:
-    if world == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{device}")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+def max_over_ranks(v: float, info) -> float:
+    from spmv_b200 import ranks
+    return ranks.max_over_ranks(v, info)
 
 
-def barrier(world: int, device: int):
-    import torch
-    torch.cuda.synchronize(device)
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier(device_ids=[device])
-        torch.cuda.synchronize(device)
+def barrier(info):
+    from spmv_b200 import ranks
+    ranks.barrier(info)
 
 
 def cpu_sample(W, D, budget_s: float, nthreads: int):
@@ -362,10 +347,10 @@ def run_reference(args, world, rank):
 # ---------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------
-def run_ours(args, world, rank, local):
+def run_ours(args, info):
     import torch
     import spmv_b200 as S
-    device = local
+    world, rank, device = info.world, info.rank, info.local
     torch.cuda.set_device(device)
     W, D, comm, cm, rm, M = setup(device)
     P = W.P
@@ -384,7 +369,7 @@ def run_ours(args, world, rank, local):
     for _ in range(args.warmup):
         _, k_its = S.cg(comm, M, bd, 10000, W.rtol, x=xd)
     clocks = ClockSampler(device)
-    barrier(world, device)
+    barrier(info)
     clocks.start()
     t_ev0 = torch.cuda.Event(enable_timing=True)
     t_ev1 = torch.cuda.Event(enable_timing=True)
@@ -396,9 +381,9 @@ def run_ours(args, world, rank, local):
     t_ev1.record(stream)
     torch.cuda.synchronize(device)
     clk = clocks.stop()
-    barrier(world, device)
+    barrier(info)
     t_local = t_ev0.elapsed_time(t_ev1) / 1e3
-    t_max = max_over_ranks(t_local, world, device)
+    t_max = max_over_ranks(t_local, info)
     value = world * args.steps / t_max
     k_mean = float(np.mean(its))
 
@@ -408,7 +393,7 @@ def run_ours(args, world, rank, local):
     xh = [torch.zeros(cm.vec_len(q), dtype=torch.float64).pin_memory().numpy()
           for q in range(P)]
     S.cg(comm, M, bh, 10000, W.rtol, x=xh)
-    barrier(world, device)
+    barrier(info)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -416,8 +401,8 @@ def run_ours(args, world, rank, local):
         S.cg(comm, M, bh, 10000, W.rtol, x=xh)
     e1.record(stream)
     torch.cuda.synchronize(device)
-    barrier(world, device)
-    te = max_over_ranks(e0.elapsed_time(e1) / 1e3, world, device)
+    barrier(info)
+    te = max_over_ranks(e0.elapsed_time(e1) / 1e3, info)
     e2e = world * args.steps / te
     h2d = int(sum(v.nbytes for v in bh))
     d2h = int(sum(D.local_sizes[q] * 8 for q in range(P)))
@@ -431,7 +416,7 @@ def run_ours(args, world, rank, local):
     for _ in range(5):
         cm.update(xs)
         M.mult(xs, out=ys)
-    barrier(world, device)
+    barrier(info)
     a0, a1, a2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
     a0.record(stream)
     for _ in range(reps):
@@ -528,16 +513,15 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    world, rank, local = dist_init()
+    info = dist_init()
     try:
         if args.impl == "reference":
-            run_reference(args, world, rank)
+            run_reference(args, info.world, info.rank)
         else:
-            run_ours(args, world, rank, local)
+            run_ours(args, info)
     finally:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        from spmv_b200 import ranks
+        ranks.finalize(info)
 
 
 if __name__ == "__main__":

@@ -130,20 +130,40 @@ void build_global_cols(spmv_matrix A) {
           "spmv: global size too large for 32-bit column indices");
   const int P = A->comm->size;
   std::vector<int32_t> g(C.nz_total, 0);
+  // 16-bit offsets from the entry's global row (rows of rank r are numbered
+  // from the sum of the earlier ranks' row counts, as in the launch tables).
+  std::vector<int16_t> d(C.nz_total, 0);
+  bool fits = d16_enabled();
+  int64_t row0 = 0;
   for (int r = 0; r < P; ++r) {
     const DevPart& D = C.parts[r];
     const int64_t ls = cm->rank[r].local_size;
     const auto& gh = cm->rank[r].ghosts;
-    for (int64_t j = 0; j < D.nnz; ++j) {
-      const int32_t c = A->h_colind[r][j];
-      g[D.nz_off + j] = c < ls ? int32_t(cm->ranges[r] + c)
-                               : int32_t(gh[size_t(c - ls)]);
+    const auto& rp = A->h_rowptr[r];
+    for (int32_t i = 0; i < D.nrows; ++i) {
+      for (int32_t j = rp[i]; j < rp[i + 1]; ++j) {
+        const int32_t c = A->h_colind[r][j];
+        const int64_t cg = c < ls ? cm->ranges[r] + c : gh[size_t(c - ls)];
+        g[D.nz_off + j] = int32_t(cg);
+        const int64_t off = cg - (row0 + i);
+        if (off < -32767 || off > 32767)
+          fits = false;
+        else
+          d[D.nz_off + j] = int16_t(off);
+      }
     }
+    row0 += D.nrows;
   }
   DeviceGuard dg(A->comm->device);
   C.cols_global.reserve(sizeof(int32_t) * C.nz_total);
   SPMVB_CUDA(cudaMemcpy(C.cols_global.ptr, g.data(), sizeof(int32_t) * C.nz_total,
                         cudaMemcpyHostToDevice));
+  C.d16 = fits && row0 < (int64_t(1) << 31) - 65536;
+  if (C.d16) {
+    C.d16_global.reserve(sizeof(int16_t) * C.nz_total);
+    SPMVB_CUDA(cudaMemcpy(C.d16_global.ptr, d.data(), sizeof(int16_t) * C.nz_total,
+                          cudaMemcpyHostToDevice));
+  }
 }
 
 // A^T per rank as its own CSR, built once by a stable counting sort over

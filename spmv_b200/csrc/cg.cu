@@ -37,6 +37,7 @@ struct CgWorkspace {
   int64_t n = 0;
   int W = 0, BS = 256;
   bool sell = false;  // K1 over the SELL-32 copy (W = loads per lane)
+  bool d16 = false;   // K1 reads 16-bit column offsets
   spmvb::DevBuf b, x, r, p, y, partials, state;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -110,7 +111,7 @@ __device__ __forceinline__ void cg_dot_finish(double acc, const CgPtrs& c,
 }
 
 // K1 over the SELL-32 copy (U loads in flight per lane).
-template <int U, int BS>
+template <int U, int BS, bool D16>
 __global__ void __launch_bounds__(BS)
     cg_spmv_dot_sell(const __grid_constant__ SpmvArgs a, const CgPtrs c,
                      cudaGraphConditionalHandle h) {
@@ -118,14 +119,14 @@ __global__ void __launch_bounds__(BS)
   if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
   const uint64_t keep = l2_policy_keep();
   double acc = 0.0;
-  sell_for_rows<double, BS, U, true>(a, [&](const PartArg& P, int row, double sum) {
+  sell_for_rows<double, BS, U, true, D16>(a, [&](const PartArg& P, int row, double sum) {
     st_pol(static_cast<double*>(P.y) + row, sum, keep);
     acc += ld_pol(static_cast<const double*>(P.xown) + row, keep) * sum;
   });
   cg_dot_finish<BS>(acc, c, smem);
 }
 
-template <int W, int BS>
+template <int W, int BS, bool D16>
 __global__ void __launch_bounds__(BS)
     cg_spmv_dot(const __grid_constant__ SpmvArgs a, const CgPtrs c,
                 cudaGraphConditionalHandle h) {
@@ -134,7 +135,7 @@ __global__ void __launch_bounds__(BS)
   // last-CTA step ever failed to run, the loop would end, never spin.
   if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
   double acc = 0.0;
-  for_rows<double, W, BS>(a, [&](const PartArg& P, int row, double sum) {
+  for_rows<double, W, BS, D16>(a, [&](const PartArg& P, int row, double sum) {
     static_cast<double*>(P.y)[row] = sum;
     acc += static_cast<const double*>(P.xown)[row] * sum;
   });
@@ -193,25 +194,27 @@ __global__ void __launch_bounds__(EW_BS) cg_update_p(const CgPtrs c) {
 }
 
 using DotFn = void (*)(SpmvArgs, CgPtrs, cudaGraphConditionalHandle);
+template <bool D16>
 DotFn dot_kernel(int W) {
   switch (W) {
-    case 1: return cg_spmv_dot<1, 256>;
-    case 2: return cg_spmv_dot<2, 256>;
-    case 4: return cg_spmv_dot<4, 256>;
-    case 8: return cg_spmv_dot<8, 256>;
-    case 16: return cg_spmv_dot<16, 256>;
-    case 32: return cg_spmv_dot<32, 256>;
+    case 1: return cg_spmv_dot<1, 256, D16>;
+    case 2: return cg_spmv_dot<2, 256, D16>;
+    case 4: return cg_spmv_dot<4, 256, D16>;
+    case 8: return cg_spmv_dot<8, 256, D16>;
+    case 16: return cg_spmv_dot<16, 256, D16>;
+    case 32: return cg_spmv_dot<32, 256, D16>;
   }
   fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: width must be 1..32, a power of two");
 }
 
+template <bool D16>
 DotFn dot_kernel_sell(int U) {
   switch (U) {
-    case 1: return cg_spmv_dot_sell<1, 256>;
-    case 2: return cg_spmv_dot_sell<2, 256>;
-    case 4: return cg_spmv_dot_sell<4, 256>;
-    case 8: return cg_spmv_dot_sell<8, 256>;
-    case 16: return cg_spmv_dot_sell<16, 256>;
+    case 1: return cg_spmv_dot_sell<1, 256, D16>;
+    case 2: return cg_spmv_dot_sell<2, 256, D16>;
+    case 4: return cg_spmv_dot_sell<4, 256, D16>;
+    case 8: return cg_spmv_dot_sell<8, 256, D16>;
+    case 16: return cg_spmv_dot_sell<16, 256, D16>;
   }
   fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: SELL width must be 1, 2, 4, 8 or 16");
 }
@@ -252,6 +255,7 @@ void build_graph(spmv_matrix A, CgWorkspace& w) {
     fill_spmv_args(sa, A->fwd, A->fwd.cols_global.as<int32_t>(), sizeof(double),
                    xs.data(), ys.data(), xown.data(), BS / W,
                    max_blocks_for(comm->num_sms, BS));
+  if (w.d16) use_d16(sa, A->fwd, w.sell);
   const int ew_grid = std::max(1, comm->num_sms) * (2048 / EW_BS);
   w.partials.reserve(sizeof(double) * std::max(sa.nblocks, ew_grid));
 
@@ -285,9 +289,9 @@ void build_graph(spmv_matrix A, CgWorkspace& w) {
   cudaGraphNode_t k1 = nullptr, k2 = nullptr, k3 = nullptr;
   if (sa.nblocks > 0) {
     void* args[] = {&sa, &c, &w.handle};
-    add_kernel(&k1, body, nullptr, 0,
-               (void*)(w.sell ? dot_kernel_sell(W) : dot_kernel(W)), sa.nblocks, BS,
-               args);
+    const DotFn fn = w.sell ? (w.d16 ? dot_kernel_sell<true>(W) : dot_kernel_sell<false>(W))
+                            : (w.d16 ? dot_kernel<true>(W) : dot_kernel<false>(W));
+    add_kernel(&k1, body, nullptr, 0, (void*)fn, sa.nblocks, BS, args);
   }
   {
     void* args[] = {&c, &w.handle};
@@ -322,6 +326,7 @@ CgWorkspace& cg_workspace(spmv_matrix A) {
     SPMVB_CUDA(cudaMemset(w->state.ptr, 0, sizeof(CgState)));
     w->sell = pick_kernel(A->kernel, A->fwd) == SPMV_KERNEL_SELL;
     if (w->sell) build_sell_global(A);
+    w->d16 = A->fwd.d16;
     w->W = A->width > 0 ? A->width
                         : (w->sell ? 8 : auto_width(A->fwd.mean_row, SPMV_FLOAT64));
     w->BS = 256;

@@ -217,6 +217,11 @@ struct DevCsr {
   bool sell_built = false;
   int64_t sl_total = 0, sz_total = 0;
   DevBuf sell_off, sell_cols, sell_vals, sell_cols_global, sell_vals32;
+  // 16-bit column offsets for the fused-halo layout (d16): entry j of
+  // global row g has column g + d16[j], built with cols_global when every
+  // offset lies in [-32767, 32767]; the SELL copy pads with -32768.
+  bool d16 = false;
+  DevBuf d16_global, sell_d16_global;
   // Row statistics (over all ranks).
   double mean_row = 0;
   int64_t max_row = 0;
@@ -285,9 +290,20 @@ void build_sell_global(spmv_matrix A);
 void build_sell_vals32(spmv_matrix A);
 // SELL launch table (the PartArg's rowptr field carries the slice offsets).
 struct SpmvArgs;
+// Plain products over a prepared launch table (vector CSR / SELL).  d16:
+// the table's cols are 16-bit offsets (see use_d16; BS must be 256).
+void launch_vector_args(const SpmvArgs& a, spmv_dtype dtype, int W, int BS,
+                        cudaStream_t s, bool d16 = false);
+void launch_sell_args(const SpmvArgs& a, spmv_dtype dtype, int U, int BS,
+                      cudaStream_t s, bool d16 = false);
 int fill_sell_args(SpmvArgs& a, const DevCsr& C, const int32_t* cols,
                    const void* vals, size_t es, const void* const* x,
                    void* const* y, const void* const* xown, int BS, int max_blocks);
+// Points a fused-halo launch table (vector CSR when !sell, else SELL) at the
+// 16-bit offsets; the kernels reinterpret the cols field.
+void use_d16(SpmvArgs& a, const DevCsr& C, bool sell);
+// Whether the solvers may use 16-bit offsets (SPMV_B200_D16=0 turns them off).
+bool d16_enabled();
 
 void build_halo_tables(spmv_l2gmap map);
 void launch_update(spmv_l2gmap map, spmv_dtype dtype, void* const* vecs,

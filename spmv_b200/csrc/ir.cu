@@ -38,7 +38,8 @@ struct IrState {
 struct IrWorkspace {
   int64_t n = 0;
   int W32 = 0, W64 = 0;
-  bool sell = false;  // products over the SELL-32 copies
+  bool sell32 = false, sell64 = false;  // products over the SELL-32 copies
+  bool d16 = false;                     // products read 16-bit column offsets
   spmvb::DevBuf b, x, r64, r, p, y, d, partials, state;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -106,17 +107,17 @@ __global__ void __launch_bounds__(EW) ir_init(const IrPtrs c, cudaGraphCondition
 }
 
 // Row traversal of the products: vector CSR (W lanes per row) or SELL-32
-// (W loads in flight per lane).
-template <typename T, int W, bool SELL, class F>
+// (W loads in flight per lane); D16: 16-bit column offsets.
+template <typename T, int W, bool SELL, bool D16, class F>
 __device__ __forceinline__ void rows_of(const SpmvArgs& a, F&& f) {
   if constexpr (SELL)
-    sell_for_rows<T, 256, W, true>(a, f);  // vectors kept in L2, matrix streamed
+    sell_for_rows<T, 256, W, true, D16>(a, f);  // vectors kept in L2, matrix streamed
   else
-    for_rows<T, W, 256>(a, f);
+    for_rows<T, W, 256, D16>(a, f);
 }
 
 // K1: y = A32 p (FP32 row sums), p.y accumulated in FP64.
-template <int W, bool SELL>
+template <int W, bool SELL, bool D16>
 __global__ void __launch_bounds__(256)
     ir_spmv_dot(const __grid_constant__ SpmvArgs a, const IrPtrs c,
                 cudaGraphConditionalHandle h_loop) {
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(256)
   if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h_loop, 0u);
   double acc = 0.0;
   const uint64_t keep = l2_policy_keep();
-  rows_of<float, W, SELL>(a, [&](const PartArg& P, int row, float sum) {
+  rows_of<float, W, SELL, D16>(a, [&](const PartArg& P, int row, float sum) {
     st_pol(static_cast<float*>(P.y) + row, sum, keep);
     acc += double(ld_pol(static_cast<const float*>(P.xown) + row, keep)) * double(sum);
   });
@@ -184,12 +185,12 @@ __global__ void __launch_bounds__(EW) ir_fold(const IrPtrs c) {
 }
 
 // Refinement 2: r64 = b - A x in FP64, and its norm.
-template <int W, bool SELL>
+template <int W, bool SELL, bool D16>
 __global__ void __launch_bounds__(256)
     ir_residual(const __grid_constant__ SpmvArgs a, const IrPtrs c) {
   __shared__ double smem[32];
   double acc = 0.0;
-  rows_of<double, W, SELL>(a, [&](const PartArg& P, int row, double sum) {
+  rows_of<double, W, SELL, D16>(a, [&](const PartArg& P, int row, double sum) {
     const int64_t g = static_cast<const double*>(P.y) - c.r64 + row;
     const double ri = c.b[g] - sum;
     c.r64[g] = ri;
@@ -258,17 +259,39 @@ __global__ void to_float(const double* __restrict__ in, float* __restrict__ out,
     out[i] = float(in[i]);
 }
 
-template <class Fn>
-Fn pick(int W, Fn f1, Fn f2, Fn f4, Fn f8, Fn f16, Fn f32) {
+using K1 = void (*)(SpmvArgs, IrPtrs, cudaGraphConditionalHandle);
+using KR = void (*)(SpmvArgs, IrPtrs);
+
+// SELL widths are loads in flight per lane (1..16), vector widths lanes per
+// row (1..32).
+template <bool SELL, bool D16>
+K1 pick_k1(int W) {
   switch (W) {
-    case 1: return f1;
-    case 2: return f2;
-    case 4: return f4;
-    case 8: return f8;
-    case 16: return f16;
-    case 32: return f32;
+    case 1: return ir_spmv_dot<1, SELL, D16>;
+    case 2: return ir_spmv_dot<2, SELL, D16>;
+    case 4: return ir_spmv_dot<4, SELL, D16>;
+    case 8: return ir_spmv_dot<8, SELL, D16>;
+    case 16: return ir_spmv_dot<16, SELL, D16>;
+    case 32: if (!SELL) return ir_spmv_dot<32, SELL, D16>;
   }
-  fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: width must be 1..32, a power of two");
+  fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: unsupported product width");
+}
+template <bool SELL, bool D16>
+KR pick_kr(int W) {
+  switch (W) {
+    case 1: return ir_residual<1, SELL, D16>;
+    case 2: return ir_residual<2, SELL, D16>;
+    case 4: return ir_residual<4, SELL, D16>;
+    case 8: return ir_residual<8, SELL, D16>;
+    case 16: return ir_residual<16, SELL, D16>;
+    case 32: if (!SELL) return ir_residual<32, SELL, D16>;
+  }
+  fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: unsupported product width");
+}
+template <class Fn>
+Fn pick4(bool sell, bool d16, int W, Fn (*ss)(int), Fn (*sp)(int), Fn (*vs)(int),
+         Fn (*vp)(int)) {
+  return sell ? (d16 ? ss(W) : sp(W)) : (d16 ? vs(W) : vp(W));
 }
 
 void add_kernel(cudaGraphNode_t* node, cudaGraph_t g, const cudaGraphNode_t* dep,
@@ -298,19 +321,66 @@ void build_ir_graph(spmv_matrix A, IrWorkspace& w) {
   const DevCsr& C = A->fwd;
   SpmvArgs a32, a64;
   const int mb = max_blocks_for(comm->num_sms, 256);
-  if (w.sell) {
-    fill_sell_args(a32, C, C.sell_cols_global.as<int32_t>(), C.sell_vals32.ptr,
-                   sizeof(float), xs32.data(), ys32.data(), own32.data(), 256, mb);
+  auto fill32 = [&](SpmvArgs& a, bool sell, int W) {
+    if (sell) {
+      fill_sell_args(a, C, C.sell_cols_global.as<int32_t>(), C.sell_vals32.ptr,
+                     sizeof(float), xs32.data(), ys32.data(), own32.data(), 256, mb);
+    } else {
+      fill_spmv_args(a, C, C.cols_global.as<int32_t>(), sizeof(float), xs32.data(),
+                     ys32.data(), own32.data(), 256 / W, mb);
+      for (int r = 0; r < P; ++r)
+        a.part[r].vals = C.vals32.as<float>() + C.parts[r].nz_off;
+    }
+    if (w.d16) use_d16(a, C, sell);
+  };
+  // The FP32 product is chosen by timing the plain FP32 kernels on the
+  // matrix (the FP64 choice does not carry over: FP32 rows are half the
+  // bytes, and the best lane count and layout differ).
+  {
+    struct Cand {
+      bool sell;
+      int w;
+    };
+    std::vector<Cand> cands;
+    for (int wv : {2, 4, 8, 16}) cands.push_back({false, wv});
+    if (C.sell_vals32.ptr)
+      for (int u : {4, 8}) cands.push_back({true, u});
+    cudaStream_t s = comm->stream;
+    cudaEvent_t e0, e1;
+    SPMVB_CUDA(cudaEventCreate(&e0));
+    SPMVB_CUDA(cudaEventCreate(&e1));
+    double best = 1e300;
+    for (const Cand& cd : cands) {
+      SpmvArgs t;
+      fill32(t, cd.sell, cd.w);
+      auto run = [&] {
+        cd.sell ? launch_sell_args(t, SPMV_FLOAT32, cd.w, 256, s, w.d16)
+                : launch_vector_args(t, SPMV_FLOAT32, cd.w, 256, s, w.d16);
+      };
+      run();
+      SPMVB_CUDA(cudaEventRecord(e0, s));
+      for (int i = 0; i < 5; ++i) run();
+      SPMVB_CUDA(cudaEventRecord(e1, s));
+      SPMVB_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      SPMVB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) {
+        best = ms;
+        w.sell32 = cd.sell;
+        w.W32 = cd.w;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  fill32(a32, w.sell32, w.W32);
+  if (w.sell64)
     fill_sell_args(a64, C, C.sell_cols_global.as<int32_t>(), C.sell_vals.ptr,
                    sizeof(double), xs64.data(), ys64.data(), nullptr, 256, mb);
-  } else {
-    fill_spmv_args(a32, C, C.cols_global.as<int32_t>(), sizeof(float), xs32.data(),
-                   ys32.data(), own32.data(), 256 / w.W32, mb);
-    for (int r = 0; r < P; ++r)
-      a32.part[r].vals = C.vals32.as<float>() + C.parts[r].nz_off;
+  else
     fill_spmv_args(a64, C, C.cols_global.as<int32_t>(), sizeof(double), xs64.data(),
                    ys64.data(), nullptr, 256 / w.W64, mb);
-  }
+  if (w.d16) use_d16(a64, C, w.sell64);
   const int ew_grid = std::max(1, comm->num_sms) * (2048 / EW);
   w.partials.reserve(sizeof(double) * 2 * std::max({a32.nblocks, a64.nblocks, ew_grid}));
 
@@ -326,26 +396,10 @@ void build_ir_graph(spmv_matrix A, IrWorkspace& w) {
   c.st = w.state.as<IrState>();
   c.n = w.n;
 
-  using K1 = void (*)(SpmvArgs, IrPtrs, cudaGraphConditionalHandle);
-  using KR = void (*)(SpmvArgs, IrPtrs);
-  K1 k1;
-  KR kr;
-  if (w.sell) {
-    // SELL widths are loads in flight per lane: 1..16.
-    k1 = pick<K1>(w.W32, ir_spmv_dot<1, true>, ir_spmv_dot<2, true>,
-                  ir_spmv_dot<4, true>, ir_spmv_dot<8, true>, ir_spmv_dot<16, true>,
-                  ir_spmv_dot<16, true>);
-    kr = pick<KR>(w.W64, ir_residual<1, true>, ir_residual<2, true>,
-                  ir_residual<4, true>, ir_residual<8, true>, ir_residual<16, true>,
-                  ir_residual<16, true>);
-  } else {
-    k1 = pick<K1>(w.W32, ir_spmv_dot<1, false>, ir_spmv_dot<2, false>,
-                  ir_spmv_dot<4, false>, ir_spmv_dot<8, false>, ir_spmv_dot<16, false>,
-                  ir_spmv_dot<32, false>);
-    kr = pick<KR>(w.W64, ir_residual<1, false>, ir_residual<2, false>,
-                  ir_residual<4, false>, ir_residual<8, false>, ir_residual<16, false>,
-                  ir_residual<32, false>);
-  }
+  const K1 k1 = pick4<K1>(w.sell32, w.d16, w.W32, pick_k1<true, true>, pick_k1<true, false>,
+                         pick_k1<false, true>, pick_k1<false, false>);
+  const KR kr = pick4<KR>(w.sell64, w.d16, w.W64, pick_kr<true, true>, pick_kr<true, false>,
+                          pick_kr<false, true>, pick_kr<false, false>);
 
   SPMVB_CUDA(cudaGraphCreate(&w.graph, 0));
   SPMVB_CUDA(cudaGraphConditionalHandleCreate(&w.h_loop, w.graph, 0,
@@ -428,16 +482,20 @@ IrWorkspace& ir_workspace(spmv_matrix A) {
     w->d.reserve(4 * n1);
     w->state.reserve(sizeof(IrState));
     SPMVB_CUDA(cudaMemset(w->state.ptr, 0, sizeof(IrState)));
-    w->sell = pick_kernel(A->kernel, A->fwd) == SPMV_KERNEL_SELL;
-    if (w->sell) {
+    // FP64 residual: the matrix's own kernel choice.  FP32 product: timed
+    // in build_ir_graph over vector CSR and (when its padding is small)
+    // SELL.
+    w->sell64 = pick_kernel(A->kernel, A->fwd) == SPMV_KERNEL_SELL;
+    if (w->sell64)
+      w->W64 = A->width > 0 ? std::min(A->width, 16) : 8;
+    else
+      w->W64 = auto_width(A->fwd.mean_row, SPMV_FLOAT64);
+    if (pick_kernel(SPMV_KERNEL_AUTO, A->fwd) == SPMV_KERNEL_SELL || w->sell64) {
       build_sell_global(A);
       build_sell_vals32(A);
-      w->W32 = A->width > 0 ? std::min(A->width, 16) : 8;
-      w->W64 = w->W32;
-    } else {
-      w->W32 = auto_width(A->fwd.mean_row, SPMV_FLOAT32);
-      w->W64 = auto_width(A->fwd.mean_row, SPMV_FLOAT64);
     }
+    w->W32 = auto_width(A->fwd.mean_row, SPMV_FLOAT32);
+    w->d16 = A->fwd.d16;
     build_ir_graph(A, *w);
     A->ir = std::move(w);
   }

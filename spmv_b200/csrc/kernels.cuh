@@ -23,6 +23,8 @@ struct PartArg {
   int32_t block_begin;
   int32_t nblocks;
   int32_t ntiles;
+  int32_t row0;            // global index of the rank's first row (16-bit
+  int32_t pad;             // column offsets are relative to the global row)
 };
 
 struct SpmvArgs {
@@ -103,6 +105,11 @@ __device__ __forceinline__ float ld_pol(const float* a, uint64_t pol) {
 __device__ __forceinline__ int ld_pol(const int* a, uint64_t pol) {
   int v;
   asm volatile("ld.global.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int ld_pol(const int16_t* a, uint64_t pol) {
+  short v;
+  asm volatile("ld.global.L2::cache_hint.s16 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(pol));
   return v;
 }
 __device__ __forceinline__ void st_pol(double* a, double v, uint64_t pol) {

@@ -8,6 +8,7 @@
 // stencils) the padding is about 1%, the row pointers are no longer read, and
 // each lane's loads are independent of each other.
 #include <algorithm>
+#include <cstdlib>
 
 #include "internal.h"
 #include "spmv_kernel.cuh"
@@ -19,14 +20,14 @@ namespace {
 inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 
 // One thread per (padded) row: copies the row's entries into its SELL
-// column and pads the rest of the slice width.
-template <typename T>
+// column and pads the rest of the slice width (column `pad`, value 0).
+template <typename T, typename CI>
 __global__ void csr_to_sell(const int32_t* __restrict__ rowptr,
-                            const int32_t* __restrict__ cols_in,
+                            const CI* __restrict__ cols_in,
                             const T* __restrict__ vals_in,
                             const int32_t* __restrict__ soff, int nrows,
-                            int nslices, int32_t* __restrict__ cols_out,
-                            T* __restrict__ vals_out) {
+                            int nslices, CI* __restrict__ cols_out,
+                            T* __restrict__ vals_out, CI pad) {
   const int64_t total = int64_t(nslices) * 32;
   for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < total;
        r += int64_t(gridDim.x) * blockDim.x) {
@@ -41,7 +42,7 @@ __global__ void csr_to_sell(const int32_t* __restrict__ rowptr,
         cols_out[idx] = cols_in[base + k];
         if (vals_out) vals_out[idx] = vals_in[base + k];
       } else {
-        cols_out[idx] = -1;
+        cols_out[idx] = pad;
         if (vals_out) vals_out[idx] = T(0);
       }
     }
@@ -56,9 +57,9 @@ __global__ void sell_to_float(const double* __restrict__ in, float* __restrict__
 }
 
 // Scatters every rank's CSR (cols_in, optional vals_in) into SELL arrays.
-void scatter_all(spmv_matrix A, DevCsr& C, const int32_t* cols_in,
-                 int32_t* cols_out, bool with_vals, cudaStream_t s) {
-  const size_t es = dtype_size(A->dtype);
+template <typename CI>
+void scatter_all(spmv_matrix A, DevCsr& C, const CI* cols_in, CI* cols_out,
+                 bool with_vals, CI pad, cudaStream_t s) {
   const int grid = std::max(1, A->comm->num_sms) * 8;
   for (size_t r = 0; r < C.parts.size(); ++r) {
     const DevPart& D = C.parts[r];
@@ -67,17 +68,18 @@ void scatter_all(spmv_matrix A, DevCsr& C, const int32_t* cols_in,
     const int32_t* rp = C.rowptr.as<int32_t>() + D.rp_off;
     const int32_t* so = C.sell_off.as<int32_t>() + D.sl_off;
     if (A->dtype == SPMV_FLOAT64) {
-      csr_to_sell<double><<<grid, 256, 0, s>>>(
+      csr_to_sell<double, CI><<<grid, 256, 0, s>>>(
           rp, cols_in + D.nz_off, C.vals.as<double>() + D.nz_off, so, D.nrows, nslices,
-          cols_out + D.sz_off, with_vals ? C.sell_vals.as<double>() + D.sz_off : nullptr);
+          cols_out + D.sz_off, with_vals ? C.sell_vals.as<double>() + D.sz_off : nullptr,
+          pad);
     } else {
-      csr_to_sell<float><<<grid, 256, 0, s>>>(
+      csr_to_sell<float, CI><<<grid, 256, 0, s>>>(
           rp, cols_in + D.nz_off, C.vals.as<float>() + D.nz_off, so, D.nrows, nslices,
-          cols_out + D.sz_off, with_vals ? C.sell_vals.as<float>() + D.sz_off : nullptr);
+          cols_out + D.sz_off, with_vals ? C.sell_vals.as<float>() + D.sz_off : nullptr,
+          pad);
     }
     SPMVB_CUDA(cudaGetLastError());
   }
-  (void)es;
 }
 
 }  // namespace
@@ -124,7 +126,8 @@ void build_sell(spmv_matrix A, DevCsr& C, cudaStream_t stream) {
                           cudaMemcpyHostToDevice));
   C.sell_cols.reserve(sizeof(int32_t) * C.sz_total);
   C.sell_vals.reserve(es * C.sz_total);
-  scatter_all(A, C, C.cols.as<int32_t>(), C.sell_cols.as<int32_t>(), true, stream);
+  scatter_all<int32_t>(A, C, C.cols.as<int32_t>(), C.sell_cols.as<int32_t>(), true, -1,
+                       stream);
   SPMVB_CUDA(cudaStreamSynchronize(stream));
   C.sell_built = true;
 }
@@ -133,8 +136,8 @@ void refresh_sell_values(spmv_matrix A) {
   DevCsr& C = A->fwd;
   if (!C.sell_built) return;
   // Same pattern: re-scatter the values (and columns, unchanged) in place.
-  scatter_all(A, C, C.cols.as<int32_t>(), C.sell_cols.as<int32_t>(), true,
-              A->comm->stream);
+  scatter_all<int32_t>(A, C, C.cols.as<int32_t>(), C.sell_cols.as<int32_t>(), true, -1,
+                       A->comm->stream);
   C.sell_vals32.release();
   SPMVB_CUDA(cudaStreamSynchronize(A->comm->stream));
 }
@@ -145,9 +148,29 @@ void build_sell_global(spmv_matrix A) {
   build_global_cols(A);
   build_sell(A, C, A->comm->stream);
   C.sell_cols_global.reserve(sizeof(int32_t) * C.sz_total);
-  scatter_all(A, C, C.cols_global.as<int32_t>(), C.sell_cols_global.as<int32_t>(), false,
-              A->comm->stream);
+  scatter_all<int32_t>(A, C, C.cols_global.as<int32_t>(), C.sell_cols_global.as<int32_t>(),
+                       false, -1, A->comm->stream);
+  if (C.d16) {
+    C.sell_d16_global.reserve(sizeof(int16_t) * C.sz_total);
+    scatter_all<int16_t>(A, C, C.d16_global.as<int16_t>(), C.sell_d16_global.as<int16_t>(),
+                         false, int16_t(-32768), A->comm->stream);
+  }
   SPMVB_CUDA(cudaStreamSynchronize(A->comm->stream));
+}
+
+bool d16_enabled() {
+  const char* v = std::getenv("SPMV_B200_D16");
+  return !(v && v[0] == '0');
+}
+
+void use_d16(SpmvArgs& a, const DevCsr& C, bool sell) {
+  require(C.d16, "spmv: no 16-bit column offsets for this matrix");
+  const int16_t* base = sell ? C.sell_d16_global.as<int16_t>() : C.d16_global.as<int16_t>();
+  require(base != nullptr, "spmv: 16-bit offsets not built for this layout");
+  for (int p = 0; p < a.nparts; ++p) {
+    const DevPart& D = C.parts[p];
+    a.part[p].cols = reinterpret_cast<const int32_t*>(base + (sell ? D.sz_off : D.nz_off));
+  }
 }
 
 void build_sell_vals32(spmv_matrix A) {
@@ -171,9 +194,12 @@ int fill_sell_args(SpmvArgs& a, const DevCsr& C, const int32_t* cols, const void
   for (const DevPart& D : C.parts)
     tiles_total += ((D.nrows + 31) / 32 + slices_per_tile - 1) / slices_per_tile;
   int blocks = 0;
+  int64_t row0 = 0;
   for (int p = 0; p < a.nparts; ++p) {
     const DevPart& D = C.parts[p];
     PartArg& P = a.part[p];
+    P.row0 = int32_t(row0);
+    row0 += D.nrows;
     P.rowptr = C.sell_off.as<int32_t>() + D.sl_off;
     P.cols = cols + D.sz_off;
     P.vals = static_cast<const char*>(vals) + D.sz_off * es;
@@ -197,19 +223,44 @@ int fill_sell_args(SpmvArgs& a, const DevCsr& C, const int32_t* cols, const void
 
 namespace {
 
-template <typename T, int BS>
+template <typename T, int BS, bool D16 = false>
 void launch_sell_u(const SpmvArgs& a, int U, cudaStream_t s) {
   switch (U) {
-    case 1: spmv_sell_kernel<T, BS, 1><<<a.nblocks, BS, 0, s>>>(a); break;
-    case 2: spmv_sell_kernel<T, BS, 2><<<a.nblocks, BS, 0, s>>>(a); break;
-    case 4: spmv_sell_kernel<T, BS, 4><<<a.nblocks, BS, 0, s>>>(a); break;
-    case 8: spmv_sell_kernel<T, BS, 8><<<a.nblocks, BS, 0, s>>>(a); break;
-    case 16: spmv_sell_kernel<T, BS, 16><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 1: spmv_sell_kernel<T, BS, 1, D16><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 2: spmv_sell_kernel<T, BS, 2, D16><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 4: spmv_sell_kernel<T, BS, 4, D16><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 8: spmv_sell_kernel<T, BS, 8, D16><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 16: spmv_sell_kernel<T, BS, 16, D16><<<a.nblocks, BS, 0, s>>>(a); break;
     default: fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: SELL width must be 1, 2, 4, 8 or 16");
   }
 }
 
 }  // namespace
+
+void launch_sell_args(const SpmvArgs& a, spmv_dtype dtype, int U, int BS,
+                      cudaStream_t stream, bool d16) {
+  if (a.nblocks == 0) return;
+  if (d16) {
+    require(BS == 256, "spmv: 16-bit offset products run 256 threads per CTA");
+    if (dtype == SPMV_FLOAT64)
+      launch_sell_u<double, 256, true>(a, U, stream);
+    else
+      launch_sell_u<float, 256, true>(a, U, stream);
+  } else if (dtype == SPMV_FLOAT64) {
+    switch (BS) {
+      case 128: launch_sell_u<double, 128>(a, U, stream); break;
+      case 256: launch_sell_u<double, 256>(a, U, stream); break;
+      default: launch_sell_u<double, 512>(a, U, stream); break;
+    }
+  } else {
+    switch (BS) {
+      case 128: launch_sell_u<float, 128>(a, U, stream); break;
+      case 256: launch_sell_u<float, 256>(a, U, stream); break;
+      default: launch_sell_u<float, 512>(a, U, stream); break;
+    }
+  }
+  SPMVB_CUDA(cudaGetLastError());
+}
 
 void launch_sell(const SpmvLaunch& L, const int32_t* sell_cols, cudaStream_t stream) {
   const DevCsr& C = *L.csr;

@@ -37,9 +37,12 @@ int fill_spmv_args(SpmvArgs& a, const DevCsr& csr, const int32_t* cols,
   for (const DevPart& D : csr.parts)
     tiles_total += (int64_t(D.nrows) + rows_per_tile - 1) / rows_per_tile;
   int blocks = 0;
+  int64_t row0 = 0;
   for (int p = 0; p < a.nparts; ++p) {
     const DevPart& D = csr.parts[p];
     PartArg& P = a.part[p];
+    P.row0 = int32_t(row0);
+    row0 += D.nrows;
     P.rowptr = csr.rowptr.as<int32_t>() + D.rp_off;
     P.cols = cols + D.nz_off;
     P.vals = static_cast<const char*>(csr.vals.ptr) + D.nz_off * es;
@@ -63,16 +66,16 @@ int fill_spmv_args(SpmvArgs& a, const DevCsr& csr, const int32_t* cols,
 
 namespace {
 
-template <typename T, int BS>
+template <typename T, int BS, bool D16 = false>
 void launch_vector(const SpmvArgs& a, int W, cudaStream_t s) {
   const dim3 grid(a.nblocks), block(BS);
   switch (W) {
-    case 1: spmv_vector_kernel<T, 1, BS><<<grid, block, 0, s>>>(a); break;
-    case 2: spmv_vector_kernel<T, 2, BS><<<grid, block, 0, s>>>(a); break;
-    case 4: spmv_vector_kernel<T, 4, BS><<<grid, block, 0, s>>>(a); break;
-    case 8: spmv_vector_kernel<T, 8, BS><<<grid, block, 0, s>>>(a); break;
-    case 16: spmv_vector_kernel<T, 16, BS><<<grid, block, 0, s>>>(a); break;
-    case 32: spmv_vector_kernel<T, 32, BS><<<grid, block, 0, s>>>(a); break;
+    case 1: spmv_vector_kernel<T, 1, BS, D16><<<grid, block, 0, s>>>(a); break;
+    case 2: spmv_vector_kernel<T, 2, BS, D16><<<grid, block, 0, s>>>(a); break;
+    case 4: spmv_vector_kernel<T, 4, BS, D16><<<grid, block, 0, s>>>(a); break;
+    case 8: spmv_vector_kernel<T, 8, BS, D16><<<grid, block, 0, s>>>(a); break;
+    case 16: spmv_vector_kernel<T, 16, BS, D16><<<grid, block, 0, s>>>(a); break;
+    case 32: spmv_vector_kernel<T, 32, BS, D16><<<grid, block, 0, s>>>(a); break;
     default: fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: width must be 1..32, a power of two");
   }
 }
@@ -88,6 +91,22 @@ void launch_vector_bs(const SpmvArgs& a, int W, int BS, cudaStream_t s) {
 }
 
 }  // namespace
+
+void launch_vector_args(const SpmvArgs& a, spmv_dtype dtype, int W, int BS,
+                        cudaStream_t s, bool d16) {
+  if (a.nblocks == 0) return;
+  if (d16) {
+    require(BS == 256, "spmv: 16-bit offset products run 256 threads per CTA");
+    if (dtype == SPMV_FLOAT64)
+      launch_vector<double, 256, true>(a, W, s);
+    else
+      launch_vector<float, 256, true>(a, W, s);
+  } else if (dtype == SPMV_FLOAT64)
+    launch_vector_bs<double>(a, W, BS, s);
+  else
+    launch_vector_bs<float>(a, W, BS, s);
+  SPMVB_CUDA(cudaGetLastError());
+}
 
 spmv_kernel pick_kernel(spmv_kernel requested, const DevCsr& C, bool allow_sell) {
   if (requested == SPMV_KERNEL_SELL) return allow_sell ? SPMV_KERNEL_SELL : SPMV_KERNEL_VECTOR;

@@ -41,9 +41,54 @@ __device__ __forceinline__ T row_dot(const int32_t* __restrict__ cols,
   return sum;
 }
 
+// As row_dot, with each column stored as a 16-bit offset from the row's
+// global index g (column = g + offset; the solvers' fused-halo layout, where
+// all offsets of a matrix fit in 16 bits).  N offsets load as one 4- or
+// 8-byte vector beside the N values.
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<double> {
+  using C = short2;
+};
+template <>
+struct Vec16<float> {
+  using C = short4;
+};
+__device__ __forceinline__ int comp(const short2& v, int i) { return i == 0 ? v.x : v.y; }
+__device__ __forceinline__ int comp(const short4& v, int i) {
+  return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+}
+
+template <typename T, int W>
+__device__ __forceinline__ T row_dot16(const int16_t* __restrict__ offs,
+                                       const T* __restrict__ vals,
+                                       const T* __restrict__ x, int g, int s, int e,
+                                       int lane) {
+  using VT = VecT<T>;
+  constexpr int N = VT::N;
+  T sum = T(0);
+  for (int j = (s & ~(N - 1)) + lane * N; j < e; j += W * N) {
+    const typename VT::V v =
+        ld_stream(reinterpret_cast<const typename VT::V*>(vals + j));
+    const typename Vec16<T>::C c =
+        ld_stream(reinterpret_cast<const typename Vec16<T>::C*>(offs + j));
+#pragma unroll
+    for (int u = 0; u < N; ++u) {
+      const int jj = j + u;
+      if (jj >= s && jj < e) sum += comp(v, u) * ld_gather(x + g + comp(c, u));
+    }
+  }
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1)
+    sum += __shfl_xor_sync(0xffffffffu, sum, o, W);
+  return sum;
+}
+
 // Visits every row of the CTA's rank: f(row, A_row . x) in lane 0 of each
-// group.  Returns nothing; the callback accumulates what it needs.
-template <typename T, int W, int BS, class F>
+// group.  Returns nothing; the callback accumulates what it needs.  D16:
+// the PartArg's cols field points to 16-bit row offsets (see row_dot16).
+template <typename T, int W, int BS, bool D16 = false, class F>
 __device__ __forceinline__ void for_rows(const SpmvArgs& a, F&& f) {
   const int p = find_part(a, blockIdx.x);
   const PartArg& P = a.part[p];
@@ -59,7 +104,12 @@ __device__ __forceinline__ void for_rows(const SpmvArgs& a, F&& f) {
       s = __ldg(P.rowptr + row);
       e = __ldg(P.rowptr + row + 1);
     }
-    const T sum = row_dot<T, W>(cols, vals, x, s, e, lane);
+    T sum;
+    if (D16)
+      sum = row_dot16<T, W>(reinterpret_cast<const int16_t*>(cols), vals, x,
+                            P.row0 + row, s, e, lane);
+    else
+      sum = row_dot<T, W>(cols, vals, x, s, e, lane);
     if (lane == 0 && row < P.nrows) f(P, row, sum);
   }
 }
@@ -75,8 +125,9 @@ __device__ __forceinline__ void for_rows(const SpmvArgs& a, F&& f) {
 //
 // KEEP (the solvers): matrix loads carry an L2 evict-first policy and the
 // x gathers an evict-last one, so vectors re-read every iteration stay in L2
-// while the matrix streams through it.
-template <typename T, int BS, int U, bool KEEP = false, class F>
+// while the matrix streams through it.  D16: 16-bit offsets from the row's
+// global index instead of 32-bit columns, -32768 marking padding.
+template <typename T, int BS, int U, bool KEEP = false, bool D16 = false, class F>
 __device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f) {
   uint64_t keep = 0, stream = 0;
   if (KEEP) {
@@ -97,6 +148,7 @@ __device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f) {
     if (slice >= nslices) continue;  // uniform across the warp
     const int o = __ldg(soff + slice);
     const int w = (__ldg(soff + slice + 1) - o) >> 5;
+    const int g = P.row0 + slice * 32 + lane;  // global row (D16 base)
     T sum = T(0);
     for (int k0 = 0; k0 < w; k0 += U) {
       T v[U];
@@ -105,13 +157,14 @@ __device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f) {
       for (int u = 0; u < U; ++u) {
         if (k0 + u < w) {
           const int idx = o + (k0 + u) * 32 + lane;
-          if (KEEP) {
-            v[u] = ld_pol(vals + idx, stream);
-            c[u] = ld_pol(cols + idx, stream);
+          if (D16) {
+            const int16_t* offs = reinterpret_cast<const int16_t*>(cols);
+            const int d = KEEP ? ld_pol(offs + idx, stream) : int(ld_stream(offs + idx));
+            c[u] = d == -32768 ? -1 : g + d;
           } else {
-            v[u] = ld_stream(vals + idx);
-            c[u] = ld_stream(cols + idx);
+            c[u] = KEEP ? ld_pol(cols + idx, stream) : ld_stream(cols + idx);
           }
+          v[u] = KEEP ? ld_pol(vals + idx, stream) : ld_stream(vals + idx);
         } else {
           v[u] = T(0);
           c[u] = -1;
@@ -134,18 +187,18 @@ __device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f) {
   }
 }
 
-template <typename T, int BS, int U>
+template <typename T, int BS, int U, bool D16 = false>
 __global__ void __launch_bounds__(BS)
     spmv_sell_kernel(const __grid_constant__ SpmvArgs a) {
-  sell_for_rows<T, BS, U>(a, [](const PartArg& P, int row, T sum) {
+  sell_for_rows<T, BS, U, false, D16>(a, [](const PartArg& P, int row, T sum) {
     static_cast<T*>(P.y)[row] = sum;
   });
 }
 
-template <typename T, int W, int BS>
+template <typename T, int W, int BS, bool D16 = false>
 __global__ void __launch_bounds__(BS)
     spmv_vector_kernel(const __grid_constant__ SpmvArgs a) {
-  for_rows<T, W, BS>(a, [](const PartArg& P, int row, T sum) {
+  for_rows<T, W, BS, D16>(a, [](const PartArg& P, int row, T sum) {
     static_cast<T*>(P.y)[row] = sum;
   });
 }

@@ -140,3 +140,29 @@ def test_matvec_demo_against_golden(cuda_device):
         norm = sum(float((psp[q][:D.local_sizes[q]] ** 2).sum()) for q in range(P))
         ref = GOLDEN["matvec_demo_N500000_apply1000"][str(P)]
         assert abs(norm - ref) <= 1e-12 * ref, (P, norm, ref)
+
+
+@pytest.mark.parametrize("cfg,scale,P,kernel", [("c2", 32, 8, "auto"), ("c2", 32, 1, "vector"),
+                                                ("c1", 64, 2, "auto")])
+def test_16bit_offsets_match_32bit_columns(cuda_device, monkeypatch, cfg, scale, P, kernel):
+    """The solvers' 16-bit column offsets change only how indices are
+    stored: FP64 CG and mixed CG give bitwise the same answers with them on
+    (default) and off (SPMV_B200_D16=0, read when the matrix's fused-halo
+    columns are first built)."""
+    W = gen.workload(cfg, scale)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("SPMV_B200_D16", flag)
+        comm, cm, rm, M, D = build(W, P)
+        if kernel != "auto":
+            M.set_kernel(kernel)
+        b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(P)]
+        x, k, _ = S.cg(comm, M, b, 10000, W.rtol, info=True)
+        xm, im = S.cg_mixed(comm, M, b, 10000, W.rtol)
+        out[flag] = (x, k, xm, im.iterations)
+    x1, k1, xm1, km1 = out["1"]
+    x0, k0, xm0, km0 = out["0"]
+    assert k1 == k0 and km1 == km0
+    for q in range(P):
+        assert np.array_equal(x1[q], x0[q])
+        assert np.array_equal(xm1[q], xm0[q])
