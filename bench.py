@@ -234,7 +234,9 @@ def run_extras(device: int, reps: int, c4_count: int):
         "mixed_solves_per_s": 1.0 / tmx, "mixed_inner_iterations": im.iterations,
         "mixed_refinements": im.refinements, "speedup": t64 / tmx,
         "relres_fp64": relres_64, "relres_mixed": relres_m,
-        "error_mixed_vs_fp64_solution": err, "kernel": tune[:3],
+        "error_mixed_vs_fp64_solution": err, "mult_kernel": tune[:3],
+        "cg_product": M.solver_product("cg"),
+        "mixed_products": [M.solver_product("mixed32"), M.solver_product("mixed64")],
         "setup_s": setup_s}
     del M, cm, b, x64, xm
     torch.cuda.empty_cache()
@@ -435,6 +437,7 @@ def run_ours(args, info):
     sb = spmv_bytes(n, nnz, P, g)
     kname, kwidth, kblock = M.get_kernel()
     kernel_fn = {"sell": "spmv_sell_kernel", "vector": "spmv_vector_kernel",
+                 "staged": "spmv_staged_kernel",
                  "merge": "merge_kernel"}.get(kname, kname)
     traffic = None
     tp = ROOT / "profiles" / "traffic.json"
@@ -444,8 +447,11 @@ def run_ours(args, info):
         except Exception:
             traffic = None
 
-    # CG iteration bytes (fused-halo layout: no ghost gather, 9 n vector terms).
+    # CG iteration bytes (fused-halo layout: no ghost gather, 9 n vector terms),
+    # counted for 32-bit CSR; the product may store its columns as 16-bit
+    # offsets, which moves 2 bytes less per nonzero than counted.
     b_iter = kernel_bytes(n, nnz, 1, 0) + 9 * n * 8
+    cg_kind, cg_w, cg_bits, cg_us = M.solver_product("cg")
     ms_per_iter = t_local / args.steps / k_mean * 1e3
 
     cpu = None
@@ -483,7 +489,9 @@ def run_ours(args, info):
                      "frac_of_8TBs": sb / t_pair / 1e9 / 8000.0},
             "cg": {"iterations": k_mean, "ms_per_iter": ms_per_iter,
                    "gbs": b_iter / (ms_per_iter / 1e3) / 1e9,
-                   "bytes_per_iter": b_iter},
+                   "bytes_per_iter": b_iter,
+                   "product": {"kernel": cg_kind, "width": cg_w, "index_bits": cg_bits,
+                               "plain_us": cg_us}},
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(args.steps * (1 + 3 * k_mean)),

@@ -68,7 +68,9 @@ typedef enum spmv_kernel {
   SPMV_KERNEL_AUTO = 0,   /* chosen from row-length statistics          */
   SPMV_KERNEL_VECTOR = 1, /* vector CSR: a W-lane group per row          */
   SPMV_KERNEL_MERGE = 2,  /* merge-path, load balanced for skewed rows   */
-  SPMV_KERNEL_SELL = 3    /* sliced ELLPACK (32-row slices), warp per slice */
+  SPMV_KERNEL_SELL = 3,   /* sliced ELLPACK (32-row slices), warp per slice */
+  SPMV_KERNEL_STAGED = 4  /* sliced ELLPACK streamed through shared memory by
+                             bulk asynchronous copies (warp-specialised)  */
 } spmv_kernel;
 
 /* Fields of the communication pattern of one rank of an L2GMap.  They are
@@ -275,6 +277,16 @@ int spmv_cg_ex(spmv_matrix A, spmv_memory memory, const double* const* b,
 /* ------------------------------------------------------------------------ */
 /* Mixed-precision CG (no counterpart in the reference; builds on spmv::cg)   */
 /* ------------------------------------------------------------------------ */
+
+/* The product a solver of this matrix runs (chosen by timing when the
+ * solver's workspace was built): solver 0 = spmv_cg, 1 = the FP32 inner
+ * product of spmv_cg_mixed, 2 = its FP64 residual product.  kernel is
+ * SPMV_KERNEL_VECTOR (width = lanes per row) or SPMV_KERNEL_SELL (width =
+ * loads in flight per lane); index_bits is 32 (global column indices) or 16
+ * (offsets from the row); us is the plain product's timed duration.  Fails
+ * when that solver has not run on the matrix.  No reference counterpart. */
+int spmv_matrix_solver_product(spmv_matrix A, int solver, spmv_kernel* kernel,
+                               int* width, int* index_bits, double* us);
 
 typedef struct spmv_ir_info {
   int iterations;   /* inner FP32 CG iterations                             */

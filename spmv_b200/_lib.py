@@ -22,7 +22,8 @@ FLOAT64, FLOAT32, COMPLEX64, COMPLEX128 = 0, 1, 2, 3
 # spmv_memory
 MEMORY_HOST, MEMORY_DEVICE = 0, 1
 # spmv_kernel
-KERNEL_AUTO, KERNEL_VECTOR, KERNEL_MERGE, KERNEL_SELL = 0, 1, 2, 3
+KERNEL_AUTO, KERNEL_VECTOR, KERNEL_MERGE, KERNEL_SELL, KERNEL_STAGED = 0, 1, 2, 3, 4
+KERNEL_NAMES = {0: "auto", 1: "vector", 2: "merge", 3: "sell", 4: "staged"}
 # spmv_pattern_field
 PATTERN_FIELDS = {"neighbours": 0, "send_count": 1, "recv_count": 2,
                   "send_offset": 3, "recv_offset": 4, "indexbuf": 5}
@@ -114,6 +115,8 @@ _SIGS = {
     "spmv_batch_set_cluster": [_p, _int],
     "spmv_batch_solve": [_p, _int, _pp, _pp, _int, C.c_double, C.POINTER(IrInfo)],
     "spmv_matrix_autotune": [_p, _int, C.POINTER(TuneResult)],
+    "spmv_matrix_solver_product": [_p, _int, C.POINTER(_int), C.POINTER(_int),
+                                   C.POINTER(_int), C.POINTER(C.c_double)],
     "spmv_matrix_mult_block": [_p, _int, _int, _pp, _pp],
     "spmv_cg_block": [_p, _int, _int, _pp, _pp, _int, C.c_double, C.POINTER(CgInfo)],
 }

@@ -34,7 +34,7 @@ LIB = PKG / "libspmv_b200.so"
 GEN = PKG / "libspmv_gen.so"
 
 CUDA_SOURCES = ["api.cpp", "l2gmap.cpp", "spmv.cu", "merge.cu", "halo.cu", "cg.cu", "ir.cu", "adjoint.cu", "sell.cu", "batch.cu", "tune.cpp", "block.cu"]
-HEADERS = ["internal.h", "kernels.cuh", "spmv_kernel.cuh"]
+HEADERS = ["internal.h", "kernels.cuh", "spmv_kernel.cuh", "sell_staged.cuh"]
 
 
 def _newer(target: Path, deps) -> bool:

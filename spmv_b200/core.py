@@ -304,7 +304,8 @@ class Matrix:
 
     def set_kernel(self, kernel: str = "auto", width: int = 0, block: int = 0) -> None:
         k = {"auto": _lib.KERNEL_AUTO, "vector": _lib.KERNEL_VECTOR,
-             "merge": _lib.KERNEL_MERGE, "sell": _lib.KERNEL_SELL}[kernel]
+             "merge": _lib.KERNEL_MERGE, "sell": _lib.KERNEL_SELL,
+             "staged": _lib.KERNEL_STAGED}[kernel]
         call("spmv_matrix_set_kernel", self._h, k, width, block)
 
     def mult_block(self, X: Sequence, out: Optional[List] = None) -> List:
@@ -329,13 +330,24 @@ class Matrix:
         returns (kernel, width, block, microseconds, candidates timed)."""
         r = _lib.TuneResult()
         call("spmv_matrix_autotune", self._h, int(reps), C.byref(r))
-        names = {0: "auto", 1: "vector", 2: "merge", 3: "sell"}
+        names = _lib.KERNEL_NAMES
         return names[r.kernel], r.width, r.block, r.us, r.candidates
+
+    def solver_product(self, solver: str = "cg"):
+        """The product a solver of this matrix runs: solver "cg", "mixed32"
+        (FP32 inner product of cg_mixed) or "mixed64" (its FP64 residual).
+        Returns (kernel, width, index_bits, microseconds of the plain
+        product); fails if that solver has not run on the matrix."""
+        s = {"cg": 0, "mixed32": 1, "mixed64": 2}[solver]
+        k, w, bits, us = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        call("spmv_matrix_solver_product", self._h, s, C.byref(k), C.byref(w),
+             C.byref(bits), C.byref(us))
+        return _lib.KERNEL_NAMES[k.value], w.value, bits.value, us.value
 
     def get_kernel(self):
         k, w, b = C.c_int(), C.c_int(), C.c_int()
         call("spmv_matrix_get_kernel", self._h, C.byref(k), C.byref(w), C.byref(b))
-        return {0: "auto", 1: "vector", 2: "merge", 3: "sell"}[k.value], w.value, b.value
+        return _lib.KERNEL_NAMES[k.value], w.value, b.value
 
     def _alloc_like(self, x0, lens):
         if _is_torch(x0):

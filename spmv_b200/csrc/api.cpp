@@ -267,7 +267,8 @@ void product(spmv_matrix A, bool transpose, spmv_memory memory,
           "spmv: unknown memory kind");
   DeviceGuard dg(comm->device);
   if (transpose) build_transpose(A);
-  if (!transpose && pick_kernel(A->kernel, A->fwd) == SPMV_KERNEL_SELL)
+  const spmv_kernel picked = pick_kernel(A->kernel, A->fwd);
+  if (!transpose && (picked == SPMV_KERNEL_SELL || picked == SPMV_KERNEL_STAGED))
     build_sell(A, A->fwd, comm->stream);
   const DevCsr& C = transpose ? A->trn : A->fwd;
   const int P = comm->size;
@@ -286,6 +287,7 @@ void product(spmv_matrix A, bool transpose, spmv_memory memory,
   L.block = A->block;
   L.num_sms = comm->num_sms;
   L.carry = transpose ? &A->trn.merge_carry : &A->fwd.merge_carry;
+  L.err = comm->wait_flag();
   cudaStream_t s = comm->stream;
   if (memory == SPMV_MEMORY_DEVICE) {
     L.x = x;
@@ -508,6 +510,14 @@ int spmv_comm_synchronize(spmv_comm comm) {
     comm->require_device();
     DeviceGuard dg(comm->device);
     SPMVB_CUDA(cudaStreamSynchronize(comm->stream));
+    if (comm->wait_err.ptr) {
+      int flag = 0;
+      SPMVB_CUDA(cudaMemcpy(&flag, comm->wait_err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+      if (flag) {
+        SPMVB_CUDA(cudaMemset(comm->wait_err.ptr, 0, sizeof(int)));
+        fail(SPMV_ERROR_CUDA, "spmv: a staged product's bounded wait timed out");
+      }
+    }
   });
 }
 
@@ -870,17 +880,21 @@ int spmv_matrix_set_kernel(spmv_matrix A, spmv_kernel kernel, int width,
   return guard([&] {
     check_mat(A);
     require(kernel == SPMV_KERNEL_AUTO || kernel == SPMV_KERNEL_VECTOR ||
-                kernel == SPMV_KERNEL_MERGE || kernel == SPMV_KERNEL_SELL,
+                kernel == SPMV_KERNEL_MERGE || kernel == SPMV_KERNEL_SELL ||
+                kernel == SPMV_KERNEL_STAGED,
             "spmv: unknown kernel");
     require(width == 0 || (width >= 1 && width <= 32 && (width & (width - 1)) == 0),
             "spmv: width must be 0 or 1..32, a power of two");
     require(kernel != SPMV_KERNEL_SELL || width <= 16,
             "spmv: SELL width (loads in flight per lane) must be 1..16");
+    require(kernel != SPMV_KERNEL_STAGED || width == 0 || width == 4 || width == 8,
+            "spmv: staged width (gathers in flight per lane) must be 4 or 8");
     require(block == 0 || block == 128 || block == 256 || block == 512,
             "spmv: block must be 0, 128, 256 or 512");
     A->kernel = kernel;
     A->width = width;
     A->block = block;
+    A->kernel_set = kernel != SPMV_KERNEL_AUTO;
     A->cg.reset();  // graphs bake the kernel choice in
     A->ir.reset();
   });
@@ -897,7 +911,9 @@ int spmv_matrix_get_kernel(spmv_matrix A, spmv_kernel* kernel, int* width,
     else if (A->width > 0)
       *width = A->width;
     else
-      *width = *kernel == SPMV_KERNEL_SELL ? 8 : auto_width(A->fwd.mean_row, A->dtype);
+      *width = (*kernel == SPMV_KERNEL_SELL || *kernel == SPMV_KERNEL_STAGED)
+                   ? 8
+                   : auto_width(A->fwd.mean_row, A->dtype);
     *block = A->block > 0 ? A->block : 256;
   });
 }
@@ -946,6 +962,22 @@ int spmv_cg(spmv_matrix A, spmv_memory memory, const double* const* b,
   const int st = spmv_cg_ex(A, memory, b, b_rows, x, max_its, rtol, &info);
   if (num_its) *num_its = info.iterations;
   return st;
+}
+
+int spmv_matrix_solver_product(spmv_matrix A, int solver, spmv_kernel* kernel, int* width,
+                               int* index_bits, double* us) {
+  return guard([&] {
+    check_mat(A);
+    require(kernel && width && index_bits && us, "spmv: NULL output");
+    require(solver >= 0 && solver <= 2, "spmv: solver must be 0, 1 or 2");
+    const SolverProduct p = solver == 0 ? cg_product(A) : ir_product(A, solver == 1);
+    *kernel = p.kind == ProductKind::Staged ? SPMV_KERNEL_STAGED
+              : p.kind == ProductKind::Sell ? SPMV_KERNEL_SELL
+                                            : SPMV_KERNEL_VECTOR;
+    *width = p.w;
+    *index_bits = p.d16 ? 16 : 32;
+    *us = p.us;
+  });
 }
 
 }  // extern "C"

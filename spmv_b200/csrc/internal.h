@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -140,6 +141,16 @@ struct spmv_comm_s {
   int refs = 1;
   // Staging buffers for SPMV_MEMORY_HOST calls.
   spmvb::DevBuf stage_in, stage_out;
+  // Device word a staged product sets when one of its bounded waits timed
+  // out (checked and cleared by spmv_comm_synchronize).
+  spmvb::DevBuf wait_err;
+  int* wait_flag() {
+    if (!wait_err.ptr) {
+      wait_err.reserve(sizeof(int));
+      SPMVB_CUDA(cudaMemset(wait_err.ptr, 0, sizeof(int)));
+    }
+    return wait_err.as<int>();
+  }
   void require_device() const {
     if (device < 0)
       spmvb::fail(SPMV_ERROR_NO_DEVICE,
@@ -222,6 +233,15 @@ struct DevCsr {
   // offset lies in [-32767, 32767]; the SELL copy pads with -32768.
   bool d16 = false;
   DevBuf d16_global, sell_d16_global;
+  // Host copy of the SELL slice offsets (all ranks, as in sell_off) and the
+  // staged-traversal tile tables, one per bytes per entry (6, 8, 10, 12):
+  // ok is false when some slice is too wide for one stage.
+  std::vector<int32_t> h_sell_off;
+  struct StagedTable {
+    bool built = false, ok = false;
+    int ntiles = 0;
+    DevBuf desc;
+  } staged[4];
   // Row statistics (over all ranks).
   double mean_row = 0;
   int64_t max_row = 0;
@@ -248,6 +268,10 @@ struct spmv_matrix_s {
   // Kernel choice.
   spmv_kernel kernel = SPMV_KERNEL_AUTO;
   int width = 0, block = 0;
+  // Set by spmv_matrix_set_kernel with an explicit kernel: the solvers'
+  // products then use that kind (and width) too.  The autotuner's choice is
+  // for mult; the solvers time their own products.
+  bool kernel_set = false;
   std::unique_ptr<CgWorkspace, void (*)(CgWorkspace*)> cg{nullptr, nullptr};
   std::unique_ptr<IrWorkspace, void (*)(IrWorkspace*)> ir{nullptr, nullptr};
 };
@@ -267,6 +291,7 @@ struct SpmvLaunch {
   int width, block;
   int num_sms;
   DevBuf* carry;                       // merge-path scratch (per matrix)
+  int* err = nullptr;                  // staged product: timed-out wait flag
 };
 void launch_spmv(const SpmvLaunch& L, cudaStream_t stream);
 void launch_merge(const SpmvLaunch& L, cudaStream_t stream, DevBuf& carry);
@@ -291,11 +316,12 @@ void build_sell_vals32(spmv_matrix A);
 // SELL launch table (the PartArg's rowptr field carries the slice offsets).
 struct SpmvArgs;
 // Plain products over a prepared launch table (vector CSR / SELL).  d16:
-// the table's cols are 16-bit offsets (see use_d16; BS must be 256).
+// the table's cols are 16-bit offsets (see use_d16); keep: the solvers' L2
+// policies (vectors kept, matrix streamed).  Either needs BS = 256.
 void launch_vector_args(const SpmvArgs& a, spmv_dtype dtype, int W, int BS,
                         cudaStream_t s, bool d16 = false);
 void launch_sell_args(const SpmvArgs& a, spmv_dtype dtype, int U, int BS,
-                      cudaStream_t s, bool d16 = false);
+                      cudaStream_t s, bool d16 = false, bool keep = false);
 int fill_sell_args(SpmvArgs& a, const DevCsr& C, const int32_t* cols,
                    const void* vals, size_t es, const void* const* x,
                    void* const* y, const void* const* xown, int BS, int max_blocks);
@@ -304,6 +330,49 @@ int fill_sell_args(SpmvArgs& a, const DevCsr& C, const int32_t* cols,
 void use_d16(SpmvArgs& a, const DevCsr& C, bool sell);
 // Whether the solvers may use 16-bit offsets (SPMV_B200_D16=0 turns them off).
 bool d16_enabled();
+// The solvers' product over the fused-halo layout: vector CSR (w lanes per
+// row) or SELL-32 (w loads in flight per lane), with 32-bit columns or
+// 16-bit offsets.
+enum class ProductKind : int {
+  Vector = 0,  // vector CSR, w lanes per row
+  Sell = 1,    // SELL-32 from registers, w loads in flight per lane
+  Staged = 2,  // SELL-32 staged in shared memory by bulk copies, w gathers per lane
+};
+struct SolverProduct {
+  ProductKind kind = ProductKind::Vector;
+  int w = 0;
+  bool d16 = false;
+  float us = 0.f;
+  bool sell_layout() const { return kind != ProductKind::Vector; }
+};
+// Launches the solver's own product kernel for a candidate over a prepared
+// launch table (the kernel's graph-only side effects compiled out).
+using ProductLauncher =
+    std::function<void(const SolverProduct&, const SpmvArgs&, cudaStream_t)>;
+// Times `launch` for each candidate (x: global input, y: global output, of
+// dtype dt; xown_rows: each rank's xown = its rows of x) and returns the
+// fastest.  A kernel set on the matrix restricts the candidates to that kind
+// and width.
+SolverProduct choose_solver_product(spmv_matrix A, spmv_dtype dt, const void* x, void* y,
+                                    bool xown_rows, const ProductLauncher& launch);
+// The products chosen by the built solver workspaces (fails if none).
+SolverProduct cg_product(spmv_matrix A);
+SolverProduct ir_product(spmv_matrix A, bool fp32);
+// Builds the SELL copies the solvers may time (when SELL is applicable).
+void prepare_solver_layouts(spmv_matrix A, bool fp32);
+// The staged tile table of the forward SELL layout for `entry_bytes` bytes per
+// entry (value + index) and `max_entries` entries per tile (built once).
+const DevCsr::StagedTable& staged_table(DevCsr& C, int entry_bytes, int max_entries);
+// Grid (persistent: at most the resident CTAs) and dynamic shared memory of
+// a staged launch of `fn` over `ntiles` tiles; sets the function's shared
+// memory limit.
+struct StagedShape {
+  int grid = 0, smem = 0;
+};
+StagedShape staged_shape(const void* fn, int entry_bytes, int ntiles, int num_sms);
+// Plain staged product over the forward SELL layout (falls back to SELL-32
+// from registers when a slice is too wide for a stage).
+void launch_staged(const SpmvLaunch& L, cudaStream_t stream);
 
 void build_halo_tables(spmv_l2gmap map);
 void launch_update(spmv_l2gmap map, spmv_dtype dtype, void* const* vecs,

@@ -25,21 +25,25 @@
 #include <algorithm>
 #include <cmath>
 
+#include <type_traits>
+
 #include "internal.h"
+#include "sell_staged.cuh"
 #include "spmv_kernel.cuh"
 
 struct IrState {
   double rr0, rr, rr_new, rr_max, alpha, beta, pap, c, rtol2, delta2, rr_true;
   double rr_prev;
-  int k, kmax, status, converged, refine, refinements, k_guard, pad1;
+  int k, kmax, status, converged, refine, refinements, k_guard, stage_err;
   unsigned int t0, t1, t2, t3, t4, pad2[3];
 };
 
 struct IrWorkspace {
   int64_t n = 0;
-  int W32 = 0, W64 = 0;
-  bool sell32 = false, sell64 = false;  // products over the SELL-32 copies
-  bool d16 = false;                     // products read 16-bit column offsets
+  spmvb::SolverProduct p32, p64;        // FP32 inner and FP64 residual products
+  const spmvb::StagedDesc* tiles32 = nullptr;  // staged tile tables (if staged)
+  const spmvb::StagedDesc* tiles64 = nullptr;
+  int ntiles32 = 0, ntiles64 = 0;
   spmvb::DevBuf b, x, r64, r, p, y, d, partials, state;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -68,6 +72,9 @@ struct IrPtrs {
   double* partials;
   IrState* st;
   int64_t n;
+  const StagedDesc* tiles32;  // staged products only
+  const StagedDesc* tiles64;
+  int ntiles32, ntiles64;
 };
 
 #define IR_LOOP(i)                                                      \
@@ -100,38 +107,54 @@ __global__ void __launch_bounds__(EW) ir_init(const IrPtrs c, cudaGraphCondition
     st->status = SPMV_SUCCESS;
     st->converged = 0;
     st->refinements = 0;
+    st->stage_err = 0;
     const bool go = st->kmax > 0 && tb > 0.0 && isfinite(tb);
     if (!go) st->converged = tb == 0.0 ? 1 : 0;
     cudaGraphSetConditional(h, go ? 1u : 0u);
   }
 }
 
-// Row traversal of the products: vector CSR (W lanes per row) or SELL-32
-// (W loads in flight per lane); D16: 16-bit column offsets.
-template <typename T, int W, bool SELL, bool D16, class F>
-__device__ __forceinline__ void rows_of(const SpmvArgs& a, F&& f) {
-  if constexpr (SELL)
-    sell_for_rows<T, 256, W, true, D16>(a, f);  // vectors kept in L2, matrix streamed
-  else
+// Row traversal of the products, by kind (ProductKind): 0 vector CSR (W
+// lanes per row), 1 SELL-32 from registers (W loads in flight per lane), 2
+// SELL-32 staged through shared memory (W gathers in flight per lane);
+// D16: 16-bit column offsets.  SELL kinds keep the vectors in L2 and stream
+// the matrix.
+template <int KIND>
+__host__ __device__ constexpr int kind_bs() {
+  return KIND == 2 ? SolverStaged::BS : 256;
+}
+template <typename T, int W, int KIND, bool D16, class F>
+__device__ __forceinline__ void rows_of(const SpmvArgs& a, const StagedDesc* tiles, int ntiles,
+                                        int* err, F&& f) {
+  if constexpr (KIND == 1) {
+    sell_for_rows<T, 256, W, true, D16>(a, f);
+  } else if constexpr (KIND == 2) {
+    using CI = typename std::conditional<D16, int16_t, int32_t>::type;
+    sell_staged_rows<SolverStaged, T, CI, W>(a, tiles, ntiles, err, f, XGather<T, true>());
+  } else {
     for_rows<T, W, 256, D16>(a, f);
+  }
 }
 
-// K1: y = A32 p (FP32 row sums), p.y accumulated in FP64.
-template <int W, bool SELL, bool D16>
-__global__ void __launch_bounds__(256)
+// K1: y = A32 p (FP32 row sums), p.y accumulated in FP64.  !H: the same
+// kernel outside the graph (no loop condition), for timing candidates.
+template <int W, int KIND, bool D16, bool H>
+__global__ void __launch_bounds__(kind_bs<KIND>())
     ir_spmv_dot(const __grid_constant__ SpmvArgs a, const IrPtrs c,
                 cudaGraphConditionalHandle h_loop) {
+  constexpr int BS = kind_bs<KIND>();
   __shared__ double smem[32];
-  if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h_loop, 0u);
+  if (H && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h_loop, 0u);
   double acc = 0.0;
   const uint64_t keep = l2_policy_keep();
-  rows_of<float, W, SELL, D16>(a, [&](const PartArg& P, int row, float sum) {
+  rows_of<float, W, KIND, D16>(a, c.tiles32, c.ntiles32, &c.st->stage_err,
+                               [&](const PartArg& P, int row, float sum) {
     st_pol(static_cast<float*>(P.y) + row, sum, keep);
     acc += double(ld_pol(static_cast<const float*>(P.xown) + row, keep)) * double(sum);
   });
-  const double part = block_sum<256>(acc, smem);
+  const double part = block_sum<BS>(acc, smem);
   double total;
-  if (grid_sum<256>(part, c.partials, &c.st->t1, &total, smem) && threadIdx.x == 0) {
+  if (grid_sum<BS>(part, c.partials, &c.st->t1, &total, smem) && threadIdx.x == 0) {
     IrState* st = c.st;
     st->pap = total;
     if (total == 0.0 || !isfinite(total)) st->status = SPMV_ERROR_BREAKDOWN;
@@ -185,20 +208,22 @@ __global__ void __launch_bounds__(EW) ir_fold(const IrPtrs c) {
 }
 
 // Refinement 2: r64 = b - A x in FP64, and its norm.
-template <int W, bool SELL, bool D16>
-__global__ void __launch_bounds__(256)
+template <int W, int KIND, bool D16>
+__global__ void __launch_bounds__(kind_bs<KIND>())
     ir_residual(const __grid_constant__ SpmvArgs a, const IrPtrs c) {
+  constexpr int BS = kind_bs<KIND>();
   __shared__ double smem[32];
   double acc = 0.0;
-  rows_of<double, W, SELL, D16>(a, [&](const PartArg& P, int row, double sum) {
+  rows_of<double, W, KIND, D16>(a, c.tiles64, c.ntiles64, &c.st->stage_err,
+                                [&](const PartArg& P, int row, double sum) {
     const int64_t g = static_cast<const double*>(P.y) - c.r64 + row;
     const double ri = c.b[g] - sum;
     c.r64[g] = ri;
     acc += ri * ri;
   });
-  const double part = block_sum<256>(acc, smem);
+  const double part = block_sum<BS>(acc, smem);
   double total;
-  if (grid_sum<256>(part, c.partials, &c.st->t3, &total, smem) && threadIdx.x == 0) {
+  if (grid_sum<BS>(part, c.partials, &c.st->t3, &total, smem) && threadIdx.x == 0) {
     IrState* st = c.st;
     st->rr_true = total;
     st->refinements += 1;
@@ -247,7 +272,7 @@ __global__ void __launch_bounds__(EW)
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     IrState* s = c.st;
     s->k_guard += 1;
-    const bool go = !stop && s->k < s->kmax && s->k_guard < s->kmax;
+    const bool go = !stop && s->k < s->kmax && s->k_guard < s->kmax && s->stage_err == 0;
     cudaGraphSetConditional(h_loop, go ? 1u : 0u);
   }
 }
@@ -262,128 +287,80 @@ __global__ void to_float(const double* __restrict__ in, float* __restrict__ out,
 using K1 = void (*)(SpmvArgs, IrPtrs, cudaGraphConditionalHandle);
 using KR = void (*)(SpmvArgs, IrPtrs);
 
-// SELL widths are loads in flight per lane (1..16), vector widths lanes per
-// row (1..32).
-template <bool SELL, bool D16>
+// Widths: vector CSR lanes per row (1..32), SELL-32 loads in flight per
+// lane (1..16), staged gathers in flight per lane (4 or 8).
+template <int KIND, bool D16, bool H>
 K1 pick_k1(int W) {
+  if (KIND == 2) return W >= 8 ? ir_spmv_dot<8, KIND, D16, H> : ir_spmv_dot<4, KIND, D16, H>;
   switch (W) {
-    case 1: return ir_spmv_dot<1, SELL, D16>;
-    case 2: return ir_spmv_dot<2, SELL, D16>;
-    case 4: return ir_spmv_dot<4, SELL, D16>;
-    case 8: return ir_spmv_dot<8, SELL, D16>;
-    case 16: return ir_spmv_dot<16, SELL, D16>;
-    case 32: if (!SELL) return ir_spmv_dot<32, SELL, D16>;
+    case 1: return ir_spmv_dot<1, KIND, D16, H>;
+    case 2: return ir_spmv_dot<2, KIND, D16, H>;
+    case 4: return ir_spmv_dot<4, KIND, D16, H>;
+    case 8: return ir_spmv_dot<8, KIND, D16, H>;
+    case 16: return ir_spmv_dot<16, KIND, D16, H>;
+    case 32: if (KIND == 0) return ir_spmv_dot<32, KIND, D16, H>;
   }
   fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: unsupported product width");
 }
-template <bool SELL, bool D16>
+template <int KIND, bool D16>
 KR pick_kr(int W) {
+  if (KIND == 2) return W >= 8 ? ir_residual<8, KIND, D16> : ir_residual<4, KIND, D16>;
   switch (W) {
-    case 1: return ir_residual<1, SELL, D16>;
-    case 2: return ir_residual<2, SELL, D16>;
-    case 4: return ir_residual<4, SELL, D16>;
-    case 8: return ir_residual<8, SELL, D16>;
-    case 16: return ir_residual<16, SELL, D16>;
-    case 32: if (!SELL) return ir_residual<32, SELL, D16>;
+    case 1: return ir_residual<1, KIND, D16>;
+    case 2: return ir_residual<2, KIND, D16>;
+    case 4: return ir_residual<4, KIND, D16>;
+    case 8: return ir_residual<8, KIND, D16>;
+    case 16: return ir_residual<16, KIND, D16>;
+    case 32: if (KIND == 0) return ir_residual<32, KIND, D16>;
   }
   fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: unsupported product width");
 }
-template <class Fn>
-Fn pick4(bool sell, bool d16, int W, Fn (*ss)(int), Fn (*sp)(int), Fn (*vs)(int),
-         Fn (*vp)(int)) {
-  return sell ? (d16 ? ss(W) : sp(W)) : (d16 ? vs(W) : vp(W));
+template <bool H>
+K1 k1_fn_h(const SolverProduct& p) {
+  switch (p.kind) {
+    case ProductKind::Vector: return p.d16 ? pick_k1<0, true, H>(p.w) : pick_k1<0, false, H>(p.w);
+    case ProductKind::Sell: return p.d16 ? pick_k1<1, true, H>(p.w) : pick_k1<1, false, H>(p.w);
+    case ProductKind::Staged: return p.d16 ? pick_k1<2, true, H>(p.w) : pick_k1<2, false, H>(p.w);
+  }
+  fail(SPMV_ERROR_INTERNAL, "spmv: unknown product kind");
+}
+K1 k1_fn(const SolverProduct& p, bool handle) {
+  return handle ? k1_fn_h<true>(p) : k1_fn_h<false>(p);
+}
+KR kr_fn(const SolverProduct& p) {
+  switch (p.kind) {
+    case ProductKind::Vector: return p.d16 ? pick_kr<0, true>(p.w) : pick_kr<0, false>(p.w);
+    case ProductKind::Sell: return p.d16 ? pick_kr<1, true>(p.w) : pick_kr<1, false>(p.w);
+    case ProductKind::Staged: return p.d16 ? pick_kr<2, true>(p.w) : pick_kr<2, false>(p.w);
+  }
+  fail(SPMV_ERROR_INTERNAL, "spmv: unknown product kind");
 }
 
-void add_kernel(cudaGraphNode_t* node, cudaGraph_t g, const cudaGraphNode_t* dep,
-                size_t ndep, void* fn, int grid, int block, void** args) {
-  cudaKernelNodeParams kp{};
-  kp.func = fn;
-  kp.gridDim = dim3(grid);
-  kp.blockDim = dim3(block);
-  kp.kernelParams = args;
-  SPMVB_CUDA(cudaGraphAddKernelNode(node, g, dep, ndep, &kp));
+// Bytes per entry of a product's matrix stream (value + index).
+int entry_bytes(const SolverProduct& p, bool fp32) {
+  return (fp32 ? 4 : 8) + (p.d16 ? 2 : 4);
+}
+const DevCsr::StagedTable& ir_tiles(spmv_matrix A, const SolverProduct& p, bool fp32) {
+  const int eb = entry_bytes(p, fp32);
+  return staged_table(A->fwd, eb, SolverStaged::max_entries(eb));
 }
 
-void build_ir_graph(spmv_matrix A, IrWorkspace& w) {
-  spmv_comm comm = A->comm;
-  const int P = comm->size;
-  const spmv_l2gmap rm = A->row_map;
-  // FP32 product over p (global layout), FP64 residual product over x.
-  std::vector<const void*> xs32(P), own32(P), xs64(P);
-  std::vector<void*> ys32(P), ys64(P);
-  for (int r = 0; r < P; ++r) {
-    xs32[r] = w.p.as<float>();
-    own32[r] = w.p.as<float>() + rm->ranges[r];
-    ys32[r] = w.y.as<float>() + rm->ranges[r];
-    xs64[r] = w.x.as<double>();
-    ys64[r] = w.r64.as<double>() + rm->ranges[r];
-  }
-  const DevCsr& C = A->fwd;
-  SpmvArgs a32, a64;
-  const int mb = max_blocks_for(comm->num_sms, 256);
-  auto fill32 = [&](SpmvArgs& a, bool sell, int W) {
-    if (sell) {
-      fill_sell_args(a, C, C.sell_cols_global.as<int32_t>(), C.sell_vals32.ptr,
-                     sizeof(float), xs32.data(), ys32.data(), own32.data(), 256, mb);
-    } else {
-      fill_spmv_args(a, C, C.cols_global.as<int32_t>(), sizeof(float), xs32.data(),
-                     ys32.data(), own32.data(), 256 / W, mb);
-      for (int r = 0; r < P; ++r)
-        a.part[r].vals = C.vals32.as<float>() + C.parts[r].nz_off;
-    }
-    if (w.d16) use_d16(a, C, sell);
-  };
-  // The FP32 product is chosen by timing the plain FP32 kernels on the
-  // matrix (the FP64 choice does not carry over: FP32 rows are half the
-  // bytes, and the best lane count and layout differ).
-  {
-    struct Cand {
-      bool sell;
-      int w;
-    };
-    std::vector<Cand> cands;
-    for (int wv : {2, 4, 8, 16}) cands.push_back({false, wv});
-    if (C.sell_vals32.ptr)
-      for (int u : {4, 8}) cands.push_back({true, u});
-    cudaStream_t s = comm->stream;
-    cudaEvent_t e0, e1;
-    SPMVB_CUDA(cudaEventCreate(&e0));
-    SPMVB_CUDA(cudaEventCreate(&e1));
-    double best = 1e300;
-    for (const Cand& cd : cands) {
-      SpmvArgs t;
-      fill32(t, cd.sell, cd.w);
-      auto run = [&] {
-        cd.sell ? launch_sell_args(t, SPMV_FLOAT32, cd.w, 256, s, w.d16)
-                : launch_vector_args(t, SPMV_FLOAT32, cd.w, 256, s, w.d16);
-      };
-      run();
-      SPMVB_CUDA(cudaEventRecord(e0, s));
-      for (int i = 0; i < 5; ++i) run();
-      SPMVB_CUDA(cudaEventRecord(e1, s));
-      SPMVB_CUDA(cudaEventSynchronize(e1));
-      float ms = 0.f;
-      SPMVB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      if (ms < best) {
-        best = ms;
-        w.sell32 = cd.sell;
-        w.W32 = cd.w;
-      }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-  }
-  fill32(a32, w.sell32, w.W32);
-  if (w.sell64)
-    fill_sell_args(a64, C, C.sell_cols_global.as<int32_t>(), C.sell_vals.ptr,
-                   sizeof(double), xs64.data(), ys64.data(), nullptr, 256, mb);
-  else
-    fill_spmv_args(a64, C, C.cols_global.as<int32_t>(), sizeof(double), xs64.data(),
-                   ys64.data(), nullptr, 256 / w.W64, mb);
-  if (w.d16) use_d16(a64, C, w.sell64);
-  const int ew_grid = std::max(1, comm->num_sms) * (2048 / EW);
-  w.partials.reserve(sizeof(double) * 2 * std::max({a32.nblocks, a64.nblocks, ew_grid}));
+// Launch shape of a product kernel: vector/SELL use the launch table's CTAs
+// (256 threads); staged runs persistent CTAs with dynamic shared memory.
+struct KShape {
+  int grid, block, smem;
+};
+KShape k_shape(const void* fn, const void* fn_graph, const SolverProduct& p, bool fp32,
+               const SpmvArgs& a, int ntiles, int num_sms) {
+  if (p.kind != ProductKind::Staged) return {a.nblocks, 256, 0};
+  const StagedShape sh = staged_shape(fn, entry_bytes(p, fp32), ntiles, num_sms);
+  if (fn_graph && fn_graph != fn)
+    SPMVB_CUDA(cudaFuncSetAttribute(fn_graph, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    sh.smem));
+  return {sh.grid, SolverStaged::BS, sh.smem};
+}
 
+IrPtrs ir_ptrs(IrWorkspace& w) {
   IrPtrs c;
   c.b = w.b.as<double>();
   c.x = w.x.as<double>();
@@ -395,11 +372,73 @@ void build_ir_graph(spmv_matrix A, IrWorkspace& w) {
   c.partials = w.partials.as<double>();
   c.st = w.state.as<IrState>();
   c.n = w.n;
+  c.tiles32 = w.tiles32;
+  c.tiles64 = w.tiles64;
+  c.ntiles32 = w.ntiles32;
+  c.ntiles64 = w.ntiles64;
+  return c;
+}
 
-  const K1 k1 = pick4<K1>(w.sell32, w.d16, w.W32, pick_k1<true, true>, pick_k1<true, false>,
-                         pick_k1<false, true>, pick_k1<false, false>);
-  const KR kr = pick4<KR>(w.sell64, w.d16, w.W64, pick_kr<true, true>, pick_kr<true, false>,
-                          pick_kr<false, true>, pick_kr<false, false>);
+void add_kernel(cudaGraphNode_t* node, cudaGraph_t g, const cudaGraphNode_t* dep,
+                size_t ndep, void* fn, int grid, int block, void** args, int smem = 0) {
+  cudaKernelNodeParams kp{};
+  kp.func = fn;
+  kp.gridDim = dim3(grid);
+  kp.blockDim = dim3(block);
+  kp.sharedMemBytes = unsigned(smem);
+  kp.kernelParams = args;
+  SPMVB_CUDA(cudaGraphAddKernelNode(node, g, dep, ndep, &kp));
+}
+
+// Launch tables of the FP32 product over p and the FP64 residual product
+// over x (global layout).
+void ir_args(spmv_matrix A, IrWorkspace& w, const SolverProduct& p, bool fp32, SpmvArgs& a) {
+  spmv_comm comm = A->comm;
+  const int P = comm->size;
+  const spmv_l2gmap rm = A->row_map;
+  std::vector<const void*> xs(P), own(P);
+  std::vector<void*> ys(P);
+  for (int r = 0; r < P; ++r) {
+    if (fp32) {
+      xs[r] = w.p.as<float>();
+      own[r] = w.p.as<float>() + rm->ranges[r];
+      ys[r] = w.y.as<float>() + rm->ranges[r];
+    } else {
+      xs[r] = w.x.as<double>();
+      ys[r] = w.r64.as<double>() + rm->ranges[r];
+    }
+  }
+  const DevCsr& C = A->fwd;
+  const int mb = max_blocks_for(comm->num_sms, 256);
+  const size_t es = fp32 ? sizeof(float) : sizeof(double);
+  const void* const* xown = fp32 ? own.data() : nullptr;
+  if (p.sell_layout()) {
+    fill_sell_args(a, C, C.sell_cols_global.as<int32_t>(),
+                   fp32 ? C.sell_vals32.ptr : C.sell_vals.ptr, es, xs.data(), ys.data(), xown,
+                   256, mb);
+  } else {
+    fill_spmv_args(a, C, C.cols_global.as<int32_t>(), es, xs.data(), ys.data(), xown,
+                   256 / p.w, mb);
+    if (fp32)
+      for (int r = 0; r < P; ++r) a.part[r].vals = C.vals32.as<float>() + C.parts[r].nz_off;
+  }
+  if (p.d16) use_d16(a, C, p.sell_layout());
+}
+
+void build_ir_graph(spmv_matrix A, IrWorkspace& w) {
+  spmv_comm comm = A->comm;
+  SpmvArgs a32, a64;
+  ir_args(A, w, w.p32, true, a32);
+  ir_args(A, w, w.p64, false, a64);
+  const K1 k1 = k1_fn(w.p32, true);
+  const KR kr = kr_fn(w.p64);
+  const KShape s1 = k_shape((const void*)k1_fn(w.p32, false), (const void*)k1, w.p32, true, a32,
+                            w.ntiles32, comm->num_sms);
+  const KShape sr = k_shape((const void*)kr, nullptr, w.p64, false, a64, w.ntiles64,
+                            comm->num_sms);
+  const int ew_grid = std::max(1, comm->num_sms) * (2048 / EW);
+  w.partials.reserve(sizeof(double) * 2 * std::max({s1.grid, sr.grid, ew_grid}));
+  IrPtrs c = ir_ptrs(w);
 
   SPMVB_CUDA(cudaGraphCreate(&w.graph, 0));
   SPMVB_CUDA(cudaGraphConditionalHandleCreate(&w.h_loop, w.graph, 0,
@@ -421,7 +460,7 @@ void build_ir_graph(spmv_matrix A, IrWorkspace& w) {
   cudaGraphNode_t b1, b2, b_if, b3;
   {
     void* args[] = {&a32, &c, &w.h_loop};
-    add_kernel(&b1, body, nullptr, 0, (void*)k1, a32.nblocks, 256, args);
+    add_kernel(&b1, body, nullptr, 0, (void*)k1, s1.grid, s1.block, args, s1.smem);
   }
   {
     void* args[] = {&c, &w.h_ref};
@@ -439,7 +478,7 @@ void build_ir_graph(spmv_matrix A, IrWorkspace& w) {
     void* a1[] = {&c};
     add_kernel(&r1, rbody, nullptr, 0, (void*)ir_fold, ew_grid, EW, a1);
     void* a2[] = {&a64, &c};
-    add_kernel(&r2, rbody, &r1, 1, (void*)kr, a64.nblocks, 256, a2);
+    add_kernel(&r2, rbody, &r1, 1, (void*)kr, sr.grid, sr.block, a2, sr.smem);
     void* a3[] = {&c};
     add_kernel(&r3, rbody, &r2, 1, (void*)ir_resync, ew_grid, EW, a3);
   }
@@ -482,24 +521,58 @@ IrWorkspace& ir_workspace(spmv_matrix A) {
     w->d.reserve(4 * n1);
     w->state.reserve(sizeof(IrState));
     SPMVB_CUDA(cudaMemset(w->state.ptr, 0, sizeof(IrState)));
-    // FP64 residual: the matrix's own kernel choice.  FP32 product: timed
-    // in build_ir_graph over vector CSR and (when its padding is small)
-    // SELL.
-    w->sell64 = pick_kernel(A->kernel, A->fwd) == SPMV_KERNEL_SELL;
-    if (w->sell64)
-      w->W64 = A->width > 0 ? std::min(A->width, 16) : 8;
-    else
-      w->W64 = auto_width(A->fwd.mean_row, SPMV_FLOAT64);
-    if (pick_kernel(SPMV_KERNEL_AUTO, A->fwd) == SPMV_KERNEL_SELL || w->sell64) {
-      build_sell_global(A);
-      build_sell_vals32(A);
-    }
-    w->W32 = auto_width(A->fwd.mean_row, SPMV_FLOAT32);
-    w->d16 = A->fwd.d16;
+    SPMVB_CUDA(cudaMemset(w->p.ptr, 0, 4 * n1));
+    SPMVB_CUDA(cudaMemset(w->x.ptr, 0, 8 * n1));
+    // Each product (FP32 inner, FP64 residual) is the candidate whose own
+    // kernel (timed outside the graph) is fastest on this matrix; the FP64
+    // choice does not carry over, FP32 rows being half the bytes.
+    prepare_solver_layouts(A, true);
+    w->partials.reserve(sizeof(double) * 2 *
+                        std::max(max_blocks_for(A->comm->num_sms, 256),
+                                 std::max(1, A->comm->num_sms) * 32));
+    IrWorkspace& ws = *w;
+    const int nsm = A->comm->num_sms;
+    auto use_tiles = [&](const SolverProduct& p, bool fp32) {
+      const StagedDesc* t = nullptr;
+      int nt = 0;
+      if (p.kind == ProductKind::Staged) {
+        const DevCsr::StagedTable& tab = ir_tiles(A, p, fp32);
+        t = tab.desc.as<StagedDesc>();
+        nt = tab.ntiles;
+      }
+      (fp32 ? ws.tiles32 : ws.tiles64) = t;
+      (fp32 ? ws.ntiles32 : ws.ntiles64) = nt;
+    };
+    auto launch = [&](const void* fn, const SolverProduct& p, bool fp32, const SpmvArgs& a,
+                      cudaStream_t s) {
+      use_tiles(p, fp32);
+      IrPtrs c = ir_ptrs(ws);
+      const KShape sh = k_shape(fn, nullptr, p, fp32, a, fp32 ? ws.ntiles32 : ws.ntiles64, nsm);
+      cudaGraphConditionalHandle none = 0;
+      void* args[] = {const_cast<SpmvArgs*>(&a), &c, &none};
+      SPMVB_CUDA(cudaLaunchKernel(fn, dim3(sh.grid), dim3(sh.block), args, size_t(sh.smem), s));
+    };
+    ws.p32 = choose_solver_product(
+        A, SPMV_FLOAT32, ws.p.ptr, ws.y.ptr, true,
+        [&](const SolverProduct& cd, const SpmvArgs& a, cudaStream_t s) {
+          launch((const void*)k1_fn(cd, false), cd, true, a, s);
+        });
+    ws.p64 = choose_solver_product(
+        A, SPMV_FLOAT64, ws.x.ptr, ws.r64.ptr, false,
+        [&](const SolverProduct& cd, const SpmvArgs& a, cudaStream_t s) {
+          launch((const void*)kr_fn(cd), cd, false, a, s);
+        });
+    use_tiles(ws.p32, true);
+    use_tiles(ws.p64, false);
     build_ir_graph(A, *w);
     A->ir = std::move(w);
   }
   return *A->ir;
+}
+
+SolverProduct ir_product(spmv_matrix A, bool fp32) {
+  require(A->ir != nullptr, "spmv: spmv_cg_mixed has not run on this matrix");
+  return fp32 ? A->ir->p32 : A->ir->p64;
 }
 
 double* ir_rhs(spmv_matrix A) { return ir_workspace(A).b.as<double>(); }
@@ -519,6 +592,8 @@ void ir_run(spmv_matrix A, int max_its, double rtol, spmv_ir_info* info) {
   SPMVB_CUDA(cudaGraphLaunch(w.exec, s));
   SPMVB_CUDA(cudaMemcpyAsync(&w.host, st, sizeof(IrState), cudaMemcpyDeviceToHost, s));
   SPMVB_CUDA(cudaStreamSynchronize(s));
+  if (w.host.stage_err)
+    fail(SPMV_ERROR_CUDA, "spmv: a staged product's bounded wait timed out");
   if (info) {
     info->iterations = w.host.k;
     info->refinements = w.host.refinements;

@@ -12,6 +12,7 @@
 
 #include "internal.h"
 #include "spmv_kernel.cuh"
+#include "sell_staged.cuh"
 
 namespace spmvb {
 
@@ -129,7 +130,51 @@ void build_sell(spmv_matrix A, DevCsr& C, cudaStream_t stream) {
   scatter_all<int32_t>(A, C, C.cols.as<int32_t>(), C.sell_cols.as<int32_t>(), true, -1,
                        stream);
   SPMVB_CUDA(cudaStreamSynchronize(stream));
+  C.h_sell_off = std::move(all_off);
   C.sell_built = true;
+}
+
+const DevCsr::StagedTable& staged_table(DevCsr& C, int entry_bytes, int max_entries) {
+  require(C.sell_built, "spmv: staged tiles need the SELL layout");
+  require(entry_bytes >= 6 && entry_bytes <= 12 && entry_bytes % 2 == 0,
+          "spmv: staged entry size must be 6, 8, 10 or 12 bytes");
+  DevCsr::StagedTable& t = C.staged[(entry_bytes - 6) / 2];
+  if (t.built) return t;
+  // Tiles of whole slices: as many consecutive slices of one rank as fit
+  // max_entries entries, at most STAGED_MAX_SLICES.
+  std::vector<StagedDesc> tiles;
+  bool ok = true;
+  for (size_t r = 0; r < C.parts.size() && ok; ++r) {
+    const DevPart& D = C.parts[r];
+    const int nslices = (D.nrows + 31) / 32;
+    const int32_t* so = C.h_sell_off.data() + D.sl_off;
+    int s = 0;
+    while (s < nslices) {
+      int e = s;
+      while (e < nslices && e - s < STAGED_MAX_SLICES && so[e + 1] - so[s] <= max_entries) ++e;
+      if (e == s) {  // one slice wider than a stage
+        ok = false;
+        break;
+      }
+      StagedDesc d{};
+      d.rank = int32_t(r);
+      d.nslices = e - s;
+      d.s0 = s;
+      d.e0 = so[s];
+      d.n = so[e] - so[s];
+      for (int j = 0; j <= e - s; ++j) d.off[j] = so[s + j] - so[s];
+      tiles.push_back(d);
+      s = e;
+    }
+  }
+  t.built = true;
+  t.ok = ok && !tiles.empty();
+  if (!t.ok) return t;
+  t.ntiles = int(tiles.size());
+  t.desc.reserve(sizeof(StagedDesc) * tiles.size());
+  SPMVB_CUDA(cudaMemcpy(t.desc.ptr, tiles.data(), sizeof(StagedDesc) * tiles.size(),
+                        cudaMemcpyHostToDevice));
+  return t;
 }
 
 void refresh_sell_values(spmv_matrix A) {
@@ -223,14 +268,14 @@ int fill_sell_args(SpmvArgs& a, const DevCsr& C, const int32_t* cols, const void
 
 namespace {
 
-template <typename T, int BS, bool D16 = false>
+template <typename T, int BS, bool D16 = false, bool KEEP = false>
 void launch_sell_u(const SpmvArgs& a, int U, cudaStream_t s) {
   switch (U) {
-    case 1: spmv_sell_kernel<T, BS, 1, D16><<<a.nblocks, BS, 0, s>>>(a); break;
-    case 2: spmv_sell_kernel<T, BS, 2, D16><<<a.nblocks, BS, 0, s>>>(a); break;
-    case 4: spmv_sell_kernel<T, BS, 4, D16><<<a.nblocks, BS, 0, s>>>(a); break;
-    case 8: spmv_sell_kernel<T, BS, 8, D16><<<a.nblocks, BS, 0, s>>>(a); break;
-    case 16: spmv_sell_kernel<T, BS, 16, D16><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 1: spmv_sell_kernel<T, BS, 1, D16, KEEP><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 2: spmv_sell_kernel<T, BS, 2, D16, KEEP><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 4: spmv_sell_kernel<T, BS, 4, D16, KEEP><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 8: spmv_sell_kernel<T, BS, 8, D16, KEEP><<<a.nblocks, BS, 0, s>>>(a); break;
+    case 16: spmv_sell_kernel<T, BS, 16, D16, KEEP><<<a.nblocks, BS, 0, s>>>(a); break;
     default: fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: SELL width must be 1, 2, 4, 8 or 16");
   }
 }
@@ -238,14 +283,20 @@ void launch_sell_u(const SpmvArgs& a, int U, cudaStream_t s) {
 }  // namespace
 
 void launch_sell_args(const SpmvArgs& a, spmv_dtype dtype, int U, int BS,
-                      cudaStream_t stream, bool d16) {
+                      cudaStream_t stream, bool d16, bool keep) {
   if (a.nblocks == 0) return;
-  if (d16) {
-    require(BS == 256, "spmv: 16-bit offset products run 256 threads per CTA");
-    if (dtype == SPMV_FLOAT64)
-      launch_sell_u<double, 256, true>(a, U, stream);
+  if (d16 || keep) {
+    require(BS == 256, "spmv: solver-form products run 256 threads per CTA");
+    const bool f64 = dtype == SPMV_FLOAT64;
+    if (d16 && keep)
+      f64 ? launch_sell_u<double, 256, true, true>(a, U, stream)
+          : launch_sell_u<float, 256, true, true>(a, U, stream);
+    else if (d16)
+      f64 ? launch_sell_u<double, 256, true, false>(a, U, stream)
+          : launch_sell_u<float, 256, true, false>(a, U, stream);
     else
-      launch_sell_u<float, 256, true>(a, U, stream);
+      f64 ? launch_sell_u<double, 256, false, true>(a, U, stream)
+          : launch_sell_u<float, 256, false, true>(a, U, stream);
   } else if (dtype == SPMV_FLOAT64) {
     switch (BS) {
       case 128: launch_sell_u<double, 128>(a, U, stream); break;
@@ -285,6 +336,63 @@ void launch_sell(const SpmvLaunch& L, const int32_t* sell_cols, cudaStream_t str
     }
   }
   SPMVB_CUDA(cudaGetLastError());
+}
+
+StagedShape staged_shape(const void* fn, int entry_bytes, int ntiles, int num_sms) {
+  StagedShape sh;
+  sh.smem = SolverStaged::smem_bytes(entry_bytes);
+  SPMVB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sh.smem));
+  int occ = 0;
+  SPMVB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, SolverStaged::BS, sh.smem));
+  require(occ > 0, "spmv: staged product does not fit on an SM");
+  sh.grid = std::max(1, std::min(ntiles, std::max(1, num_sms) * occ));
+  return sh;
+}
+
+namespace {
+
+template <typename T, typename CI, int U>
+__global__ void __launch_bounds__(SolverStaged::BS)
+    spmv_staged_kernel(const __grid_constant__ SpmvArgs a, const StagedDesc* tiles, int ntiles,
+                       int* err) {
+  sell_staged_rows<SolverStaged, T, CI, U>(
+      a, tiles, ntiles, err,
+      [](const PartArg& P, int row, T sum) { static_cast<T*>(P.y)[row] = sum; }, XGather<T>());
+}
+
+template <typename T>
+void launch_staged_t(const SpmvLaunch& L, const SpmvArgs& a, const DevCsr::StagedTable& t,
+                     int U, cudaStream_t s) {
+  const void* fn = U >= 8 ? (const void*)spmv_staged_kernel<T, int32_t, 8>
+                          : (const void*)spmv_staged_kernel<T, int32_t, 4>;
+  const StagedShape sh = staged_shape(fn, int(sizeof(T)) + 4, t.ntiles, L.num_sms);
+  const StagedDesc* tiles = t.desc.as<StagedDesc>();
+  int ntiles = t.ntiles;
+  int* err = L.err;
+  void* args[] = {const_cast<SpmvArgs*>(&a), &tiles, &ntiles, &err};
+  SPMVB_CUDA(cudaLaunchKernel(fn, dim3(sh.grid), dim3(SolverStaged::BS), args, size_t(sh.smem), s));
+}
+
+}  // namespace
+
+void launch_staged(const SpmvLaunch& L, cudaStream_t stream) {
+  DevCsr& C = const_cast<DevCsr&>(*L.csr);
+  require(C.sell_built, "spmv: staged product needs the SELL layout");
+  const size_t es = dtype_size(L.dtype);
+  const int eb = int(es) + 4;
+  const DevCsr::StagedTable& t = staged_table(C, eb, SolverStaged::max_entries(eb));
+  if (!t.ok) {
+    launch_sell(L, C.sell_cols.as<int32_t>(), stream);
+    return;
+  }
+  SpmvArgs a;
+  fill_sell_args(a, C, C.sell_cols.as<int32_t>(), C.sell_vals.ptr, es, L.x, L.y, nullptr, 256,
+                 max_blocks_for(L.num_sms, 256));
+  const int U = L.width > 0 ? L.width : 8;
+  if (L.dtype == SPMV_FLOAT64)
+    launch_staged_t<double>(L, a, t, U, stream);
+  else
+    launch_staged_t<float>(L, a, t, U, stream);
 }
 
 }  // namespace spmvb

@@ -1,0 +1,269 @@
+// SELL-32 traversal with the matrix stream staged in shared memory by bulk
+// asynchronous copies (cp.async.bulk, completion counted on mbarriers), in a
+// warp-specialised pipeline.
+//
+// The rows of a matrix are cut into tiles of whole slices (a host-built
+// table of StagedDesc; at most STAGED_MAX_SLICES slices and
+// CFG::max_entries entries per tile).  A
+// persistent CTA takes tiles blockIdx.x, blockIdx.x + gridDim.x, ...:
+//
+//   producer warp (the last warp, one lane): for each tile, waits until the
+//     consumers have released the stage buffer and issues three bulk copies
+//     that complete on the stage's "full" barrier: the tile's descriptor
+//     (rank, slice count, slice offsets) as the stage header, its values and
+//     its column indices (or 16-bit offsets), both contiguous in the SELL
+//     arrays;
+//   consumer warps (STAGED_CONSUMERS): wait for the stage, take their share
+//     of its slices (dealt round robin over the CTA's sequence of slices; one
+//     lane per row), read the entries from shared memory
+//     (consecutive lanes, consecutive words), gather x from global memory
+//     (L2), sum each row in storage order, call f, and release the stage.
+//
+// Consumers never wait on global loads for metadata, and the matrix bytes in
+// flight per SM are set by the stage buffers rather than by registers.  Rows
+// are summed in the same order as sell_for_rows, so results match that
+// traversal bit for bit.
+//
+// Every wait is bounded: a barrier that does not complete within the limit
+// sets *err and ends that warp's loop; the producer then waits (bounded
+// again) for the copies it issued, so no copy is left writing to the shared
+// memory of a finished CTA.
+#pragma once
+
+#include "spmv_kernel.cuh"
+
+namespace spmvb {
+
+constexpr int STAGED_HEADER_BYTES = 128;
+constexpr int STAGED_MAX_SLICES = 16;
+
+// Pipeline shape: NC consumer warps (+ one producer warp), STAGES tiles in
+// flight per CTA, DATA bytes of values + indices per tile.
+template <int NC_, int STAGES_, int DATA_>
+struct StagedCfg {
+  static constexpr int NC = NC_;
+  static constexpr int STAGES = STAGES_;
+  static constexpr int DATA = DATA_;
+  static constexpr int BS = 32 * (NC + 1);
+  // Entries of one stage for `eb` bytes per entry (a multiple of 32).
+  __host__ __device__ static constexpr int max_entries(int eb) { return (DATA / eb) / 32 * 32; }
+  __host__ __device__ static constexpr int stage_bytes(int eb) {
+    return STAGED_HEADER_BYTES + max_entries(eb) * eb;
+  }
+  // Dynamic shared memory of a launch.
+  __host__ __device__ static constexpr int smem_bytes(int eb) { return STAGES * stage_bytes(eb); }
+};
+
+// The shape the solvers' products use: 12 consumer warps, 4 stages of 16 KB
+// (3 CTAs per SM), measured best of the shapes tried on the 7-point stencil
+// in FP64 and FP32.
+using SolverStaged = StagedCfg<12, 4, 16384>;
+
+// Descriptor of one tile (host-built, 128 bytes, copied as the stage's
+// header): slices [s0, s0 + nslices) of rank `rank`, whose entries start at
+// entry e0 of the rank's SELL arrays and number n; off[j] = first entry of
+// slice s0 + j relative to e0 (off[nslices] = n).
+struct StagedDesc {
+  int32_t rank, nslices, s0, e0;
+  int32_t n, pad[3];
+  int32_t off[24];
+};
+static_assert(sizeof(StagedDesc) == STAGED_HEADER_BYTES, "staged descriptor is one header");
+static_assert(STAGED_MAX_SLICES + 1 <= 24, "staged descriptor too small");
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// One probe of the barrier's phase (the instruction itself suspends for a
+// bounded, hardware-defined time); true once phase `parity` has completed.
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for phase `parity` of `bar`, giving up after a bounded number of
+// probes (seconds; a healthy pipeline needs microseconds).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < (1u << 22); ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Bulk copy global -> shared, completion counted on `bar`; the source gets
+// an L2 evict-first policy (the matrix is read once per product).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar, uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1], %2, [%3], %4;" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
+      : "memory");
+}
+
+// Traversal.  CI: int32_t (columns, -1 = padding) or int16_t (offsets from
+// the global row g = row0 + row, -32768 = padding).  U: gathers in flight
+// per lane; gx(P, c): the gathered vector (XGather: the PartArg's x).
+// f(P, row, sum) is called by the lane owning each row.  All CFG::BS
+// threads must call this (block-wide reductions may follow).
+template <class CFG, typename T, typename CI, int U, class F, class G>
+__device__ __forceinline__ void sell_staged_rows(const SpmvArgs& a,
+                                                 const StagedDesc* __restrict__ tiles,
+                                                 int ntiles, int* err, F&& f, const G& gx) {
+  constexpr int STAGED_STAGES = CFG::STAGES;
+  constexpr int STAGED_CONSUMERS = CFG::NC;
+  constexpr int EB = int(sizeof(T) + sizeof(CI));
+  constexpr int MAXE = CFG::max_entries(EB);
+  constexpr int STAGE = CFG::stage_bytes(EB);
+  extern __shared__ __align__(128) unsigned char staged_smem[];
+  __shared__ __align__(8) uint64_t full[STAGED_STAGES], empty[STAGED_STAGES];
+
+  const int tid = int(threadIdx.x);
+  const int warp = tid >> 5, lane = tid & 31;
+  const int count = int(blockIdx.x) < ntiles
+                        ? (ntiles - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x)
+                        : 0;
+  auto header = [&](int st) {
+    return reinterpret_cast<const StagedDesc*>(staged_smem + st * STAGE);
+  };
+  auto stage_vals = [&](int st) {
+    return reinterpret_cast<T*>(staged_smem + st * STAGE + STAGED_HEADER_BYTES);
+  };
+  auto stage_cols = [&](int st) {
+    return reinterpret_cast<CI*>(staged_smem + st * STAGE + STAGED_HEADER_BYTES +
+                                 MAXE * int(sizeof(T)));
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < STAGED_STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], STAGED_CONSUMERS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  if (warp == STAGED_CONSUMERS) {
+    // Producer.  The next tile's rank, e0 and n are loaded one tile ahead,
+    // so no issue waits on a global load.
+    if (lane == 0) {
+      const uint64_t stream = l2_policy_stream();
+      int issued = 0;
+      bool failed = false;
+      int4 nxt = make_int4(0, 0, 0, 0);  // rank, e0, n of tile i
+      if (count > 0) {
+        const StagedDesc* d = tiles + blockIdx.x;
+        nxt = make_int4(__ldg(&d->rank), __ldg(&d->e0), __ldg(&d->n), 0);
+      }
+      for (int i = 0; i < count; ++i) {
+        const int st = i % STAGED_STAGES;
+        const int4 cur = nxt;
+        if (i + 1 < count) {
+          const StagedDesc* d = tiles + int(blockIdx.x) + (i + 1) * int(gridDim.x);
+          nxt = make_int4(__ldg(&d->rank), __ldg(&d->e0), __ldg(&d->n), 0);
+        }
+        if (i >= STAGED_STAGES &&
+            !mbar_wait_bounded(&empty[st], uint32_t(i / STAGED_STAGES - 1) & 1u)) {
+          failed = true;
+          break;
+        }
+        const PartArg& P = a.part[cur.x];
+        const uint32_t n = uint32_t(cur.z);
+        mbar_arrive_expect_tx(&full[st], STAGED_HEADER_BYTES + n * uint32_t(EB));
+        bulk_g2s(staged_smem + st * STAGE, tiles + int(blockIdx.x) + i * int(gridDim.x),
+                 STAGED_HEADER_BYTES, &full[st], stream);
+        if (n > 0) {
+          bulk_g2s(stage_vals(st), static_cast<const T*>(P.vals) + cur.y,
+                   n * uint32_t(sizeof(T)), &full[st], stream);
+          bulk_g2s(stage_cols(st), reinterpret_cast<const CI*>(P.cols) + cur.y,
+                   n * uint32_t(sizeof(CI)), &full[st], stream);
+        }
+        issued = i + 1;
+      }
+      if (failed) {
+        if (err) atomicExch(err, 1);
+        // Wait (bounded) for the last STAGES tiles issued to land.
+        for (int i = issued - STAGED_STAGES < 0 ? 0 : issued - STAGED_STAGES; i < issued; ++i)
+          mbar_wait_bounded(&full[i % STAGED_STAGES], uint32_t(i / STAGED_STAGES) & 1u);
+      }
+    }
+    return;
+  }
+
+  // Consumers.  Slices are dealt round robin over the CTA's whole sequence
+  // of tiles (q0 = slices in the tiles before this one), so a tile with
+  // fewer slices than consumer warps leaves no warp idle for long.
+  int q0 = 0;
+  for (int i = 0; i < count; ++i) {
+    const int st = i % STAGED_STAGES;
+    if (!mbar_wait_bounded(&full[st], uint32_t(i / STAGED_STAGES) & 1u)) {
+      if (err && lane == 0) atomicExch(err, 1);
+      break;
+    }
+    const StagedDesc* h = header(st);
+    const PartArg& P = a.part[h->rank];
+    const T* sv = stage_vals(st);
+    const CI* sc = stage_cols(st);
+    const int ns = h->nslices;
+    const int j0 = ((warp - q0) % STAGED_CONSUMERS + STAGED_CONSUMERS) % STAGED_CONSUMERS;
+    q0 += ns;
+    for (int j = j0; j < ns; j += STAGED_CONSUMERS) {
+      const int o = h->off[j];
+      const int w = (h->off[j + 1] - o) >> 5;
+      const int row = (h->s0 + j) * 32 + lane;
+      const int g = P.row0 + row;
+      T sum = T(0);
+      for (int k0 = 0; k0 < w; k0 += U) {
+        T v[U], xv[U];
+        bool ok[U];
+        int c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const bool in = k0 + u < w;
+          const int idx = o + (k0 + u) * 32 + lane;
+          const int ci = in ? int(sc[idx]) : 0;
+          v[u] = in ? sv[idx] : T(0);
+          if (sizeof(CI) == 2) {
+            ok[u] = in && ci != -32768;
+            c[u] = g + ci;
+          } else {
+            ok[u] = in && ci >= 0;
+            c[u] = ci;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) xv[u] = ok[u] ? gx(P, c[u]) : T(0);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (ok[u]) sum += v[u] * xv[u];
+      }
+      if (row < P.nrows) f(P, row, sum);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[st]);
+  }
+}
+
+}  // namespace spmvb

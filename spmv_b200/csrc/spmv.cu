@@ -15,6 +15,7 @@
 
 #include "internal.h"
 #include "spmv_kernel.cuh"
+#include "sell_staged.cuh"
 
 namespace spmvb {
 
@@ -108,8 +109,127 @@ void launch_vector_args(const SpmvArgs& a, spmv_dtype dtype, int W, int BS,
   SPMVB_CUDA(cudaGetLastError());
 }
 
+void prepare_solver_layouts(spmv_matrix A, bool fp32) {
+  build_global_cols(A);
+  if (fp32) ensure_vals32(A);
+  const bool sell_ok = pick_kernel(SPMV_KERNEL_AUTO, A->fwd) == SPMV_KERNEL_SELL;
+  const bool want = A->kernel_set
+                        ? (A->kernel == SPMV_KERNEL_SELL || A->kernel == SPMV_KERNEL_STAGED)
+                        : sell_ok;
+  if (want) {
+    build_sell_global(A);
+    if (fp32) build_sell_vals32(A);
+  }
+}
+
+SolverProduct choose_solver_product(spmv_matrix A, spmv_dtype dt, const void* x, void* y,
+                                    bool xown_rows, const ProductLauncher& launch) {
+  const DevCsr& C = A->fwd;
+  spmv_comm comm = A->comm;
+  const int P = comm->size;
+  const bool f32 = dt == SPMV_FLOAT32;
+  const size_t es = f32 ? sizeof(float) : sizeof(double);
+  const void* sell_vals = f32 ? C.sell_vals32.ptr : C.sell_vals.ptr;
+  const bool have_sell = C.sell_cols_global.ptr != nullptr && sell_vals != nullptr;
+
+  std::vector<SolverProduct> cands;
+  const bool only = A->kernel_set;
+  const spmv_kernel k = A->kernel;
+  const bool want_vec = !only || !have_sell || (k != SPMV_KERNEL_SELL && k != SPMV_KERNEL_STAGED);
+  const bool want_sell = have_sell && (!only || k == SPMV_KERNEL_SELL);
+  const bool want_staged = have_sell && (!only || k == SPMV_KERNEL_STAGED);
+  std::vector<bool> d16s{false};
+  if (C.d16) d16s.push_back(true);
+  for (bool d : d16s) {
+    if (want_vec) {
+      std::vector<int> ws;
+      if (only && k == SPMV_KERNEL_VECTOR && A->width > 0) {
+        ws.push_back(A->width);
+      } else {
+        const int aw = auto_width(C.mean_row, dt);
+        for (int w : {aw / 2, aw, aw * 2})
+          if (w >= 1 && w <= 32 && std::find(ws.begin(), ws.end(), w) == ws.end())
+            ws.push_back(w);
+      }
+      for (int w : ws) cands.push_back({ProductKind::Vector, w, d, 0.f});
+    }
+    if (want_sell) {
+      if (only && A->width > 0)
+        cands.push_back({ProductKind::Sell, std::min(A->width, 16), d, 0.f});
+      else
+        for (int u : {2, 4, 8}) cands.push_back({ProductKind::Sell, u, d, 0.f});
+    }
+    if (want_staged) {
+      const int eb = int(es) + (d ? 2 : 4);
+      if (staged_table(A->fwd, eb, SolverStaged::max_entries(eb)).ok) {
+        if (only && A->width > 0)
+          cands.push_back({ProductKind::Staged, A->width >= 8 ? 8 : 4, d, 0.f});
+        else
+          for (int u : {4, 8}) cands.push_back({ProductKind::Staged, u, d, 0.f});
+      }
+    }
+  }
+  require(!cands.empty(), "spmv: no product kernel applies to this matrix");
+
+  const spmv_l2gmap rm = A->row_map;
+  std::vector<const void*> xs(P), own(P);
+  std::vector<void*> ys(P);
+  for (int r = 0; r < P; ++r) {
+    xs[r] = x;
+    own[r] = static_cast<const char*>(x) + rm->ranges[r] * es;
+    ys[r] = static_cast<char*>(y) + rm->ranges[r] * es;
+  }
+  const void* const* xown = xown_rows ? own.data() : nullptr;
+  const int mb = max_blocks_for(comm->num_sms, 256);
+  cudaStream_t s = comm->stream;
+  cudaEvent_t e0, e1;
+  SPMVB_CUDA(cudaEventCreate(&e0));
+  SPMVB_CUDA(cudaEventCreate(&e1));
+  SolverProduct best = cands.front();
+  best.us = 1e30f;
+  static const char* names[] = {"vector", "sell", "staged"};
+  try {
+    for (SolverProduct& cd : cands) {
+      SpmvArgs a;
+      if (cd.sell_layout()) {
+        fill_sell_args(a, C, C.sell_cols_global.as<int32_t>(), sell_vals, es, xs.data(),
+                       ys.data(), xown, 256, mb);
+      } else {
+        fill_spmv_args(a, C, C.cols_global.as<int32_t>(), es, xs.data(), ys.data(), xown,
+                       256 / cd.w, mb);
+        if (f32)
+          for (int r = 0; r < P; ++r)
+            a.part[r].vals = C.vals32.as<float>() + C.parts[r].nz_off;
+      }
+      if (cd.d16) use_d16(a, C, cd.sell_layout());
+      auto run = [&] { launch(cd, a, s); };
+      run();
+      constexpr int reps = 5;
+      SPMVB_CUDA(cudaEventRecord(e0, s));
+      for (int i = 0; i < reps; ++i) run();
+      SPMVB_CUDA(cudaEventRecord(e1, s));
+      SPMVB_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      SPMVB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      cd.us = ms * 1000.f / reps;
+      if (cd.us < best.us) best = cd;
+      debug_log(std::string("solver product ") + (f32 ? "f32 " : "f64 ") +
+                names[int(cd.kind)] + " " + std::to_string(cd.w) +
+                (cd.d16 ? " d16 " : " d32 ") + std::to_string(cd.us) + " us");
+    }
+  } catch (...) {
+    soft_check(cudaEventDestroy(e0), "cudaEventDestroy");
+    soft_check(cudaEventDestroy(e1), "cudaEventDestroy");
+    throw;
+  }
+  soft_check(cudaEventDestroy(e0), "cudaEventDestroy");
+  soft_check(cudaEventDestroy(e1), "cudaEventDestroy");
+  return best;
+}
+
 spmv_kernel pick_kernel(spmv_kernel requested, const DevCsr& C, bool allow_sell) {
-  if (requested == SPMV_KERNEL_SELL) return allow_sell ? SPMV_KERNEL_SELL : SPMV_KERNEL_VECTOR;
+  if (requested == SPMV_KERNEL_SELL || requested == SPMV_KERNEL_STAGED)
+    return allow_sell ? requested : SPMV_KERNEL_VECTOR;
   if (requested != SPMV_KERNEL_AUTO) return requested;
   const double skew_limit = std::max(64.0, 8.0 * C.mean_row);
   if (double(C.max_row) > skew_limit) return SPMV_KERNEL_MERGE;
@@ -143,6 +263,10 @@ void launch_spmv(const SpmvLaunch& L, cudaStream_t stream) {
   }
   if (k == SPMV_KERNEL_SELL) {
     launch_sell(L, L.csr->sell_cols.as<int32_t>(), stream);
+    return;
+  }
+  if (k == SPMV_KERNEL_STAGED) {
+    launch_staged(L, stream);
     return;
   }
   SpmvArgs a;

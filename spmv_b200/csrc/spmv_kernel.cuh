@@ -14,13 +14,26 @@ int fill_spmv_args(SpmvArgs& a, const DevCsr& csr, const int32_t* cols,
                    const void* const* xown, int rows_per_tile,
                    int max_blocks);
 
-// Dot product of one CSR row with x, computed by a group of W lanes.  The
-// result is identical in every lane of the group.
-template <typename T, int W>
+// Gathers: g(P, c) returns entry c of the vector a rank's product reads.
+// XGather loads the PartArg's x (KEEP: with the L2 evict-last policy, for
+// solver vectors re-read every iteration); a solver may pass its own (the
+// CG product forms p = r + beta p_old on the fly).
+template <typename T, bool KEEP = false>
+struct XGather {
+  uint64_t pol;
+  __device__ __forceinline__ XGather() : pol(KEEP ? l2_policy_keep() : 0) {}
+  __device__ __forceinline__ T operator()(const PartArg& P, int c) const {
+    const T* x = static_cast<const T*>(P.x);
+    return KEEP ? ld_pol(x + c, pol) : ld_gather(x + c);
+  }
+};
+
+// Dot product of one CSR row with the gathered vector, computed by a group
+// of W lanes.  The result is identical in every lane of the group.
+template <typename T, int W, class G>
 __device__ __forceinline__ T row_dot(const int32_t* __restrict__ cols,
-                                     const T* __restrict__ vals,
-                                     const T* __restrict__ x, int s, int e,
-                                     int lane) {
+                                     const T* __restrict__ vals, const PartArg& P,
+                                     const G& gx, int s, int e, int lane) {
   using VT = VecT<T>;
   constexpr int N = VT::N;
   T sum = T(0);
@@ -32,7 +45,7 @@ __device__ __forceinline__ T row_dot(const int32_t* __restrict__ cols,
 #pragma unroll
     for (int u = 0; u < N; ++u) {
       const int jj = j + u;
-      if (jj >= s && jj < e) sum += comp(v, u) * ld_gather(x + comp(c, u));
+      if (jj >= s && jj < e) sum += comp(v, u) * gx(P, comp(c, u));
     }
   }
 #pragma unroll
@@ -60,11 +73,10 @@ __device__ __forceinline__ int comp(const short4& v, int i) {
   return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
 }
 
-template <typename T, int W>
+template <typename T, int W, class G>
 __device__ __forceinline__ T row_dot16(const int16_t* __restrict__ offs,
-                                       const T* __restrict__ vals,
-                                       const T* __restrict__ x, int g, int s, int e,
-                                       int lane) {
+                                       const T* __restrict__ vals, const PartArg& P,
+                                       const G& gx, int g, int s, int e, int lane) {
   using VT = VecT<T>;
   constexpr int N = VT::N;
   T sum = T(0);
@@ -76,7 +88,7 @@ __device__ __forceinline__ T row_dot16(const int16_t* __restrict__ offs,
 #pragma unroll
     for (int u = 0; u < N; ++u) {
       const int jj = j + u;
-      if (jj >= s && jj < e) sum += comp(v, u) * ld_gather(x + g + comp(c, u));
+      if (jj >= s && jj < e) sum += comp(v, u) * gx(P, g + comp(c, u));
     }
   }
 #pragma unroll
@@ -88,13 +100,12 @@ __device__ __forceinline__ T row_dot16(const int16_t* __restrict__ offs,
 // Visits every row of the CTA's rank: f(row, A_row . x) in lane 0 of each
 // group.  Returns nothing; the callback accumulates what it needs.  D16:
 // the PartArg's cols field points to 16-bit row offsets (see row_dot16).
-template <typename T, int W, int BS, bool D16 = false, class F>
-__device__ __forceinline__ void for_rows(const SpmvArgs& a, F&& f) {
+template <typename T, int W, int BS, bool D16 = false, class F, class G = XGather<T>>
+__device__ __forceinline__ void for_rows(const SpmvArgs& a, F&& f, const G& gx = G()) {
   const int p = find_part(a, blockIdx.x);
   const PartArg& P = a.part[p];
   const int32_t* __restrict__ cols = P.cols;
   const T* __restrict__ vals = static_cast<const T*>(P.vals);
-  const T* __restrict__ x = static_cast<const T*>(P.x);
   const int group = int(threadIdx.x) / W, lane = int(threadIdx.x) % W;
   for (int tile = int(blockIdx.x) - P.block_begin; tile < P.ntiles;
        tile += P.nblocks) {
@@ -106,10 +117,10 @@ __device__ __forceinline__ void for_rows(const SpmvArgs& a, F&& f) {
     }
     T sum;
     if (D16)
-      sum = row_dot16<T, W>(reinterpret_cast<const int16_t*>(cols), vals, x,
+      sum = row_dot16<T, W>(reinterpret_cast<const int16_t*>(cols), vals, P, gx,
                             P.row0 + row, s, e, lane);
     else
-      sum = row_dot<T, W>(cols, vals, x, s, e, lane);
+      sum = row_dot<T, W>(cols, vals, P, gx, s, e, lane);
     if (lane == 0 && row < P.nrows) f(P, row, sum);
   }
 }
@@ -124,22 +135,19 @@ __device__ __forceinline__ void for_rows(const SpmvArgs& a, F&& f) {
 // order (k ascending), the order of the sequential CSR loop.
 //
 // KEEP (the solvers): matrix loads carry an L2 evict-first policy and the
-// x gathers an evict-last one, so vectors re-read every iteration stay in L2
-// while the matrix streams through it.  D16: 16-bit offsets from the row's
+// default gathers an evict-last one, so vectors re-read every iteration stay
+// in L2 while the matrix streams through it.  D16: 16-bit offsets from the row's
 // global index instead of 32-bit columns, -32768 marking padding.
-template <typename T, int BS, int U, bool KEEP = false, bool D16 = false, class F>
-__device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f) {
-  uint64_t keep = 0, stream = 0;
-  if (KEEP) {
-    keep = l2_policy_keep();
-    stream = l2_policy_stream();
-  }
+template <typename T, int BS, int U, bool KEEP = false, bool D16 = false, class F,
+          class G = XGather<T, KEEP>>
+__device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f, const G& gx = G()) {
+  uint64_t stream = 0;
+  if (KEEP) stream = l2_policy_stream();
   const int p = find_part(a, blockIdx.x);
   const PartArg& P = a.part[p];
   const int32_t* __restrict__ soff = P.rowptr;
   const int32_t* __restrict__ cols = P.cols;
   const T* __restrict__ vals = static_cast<const T*>(P.vals);
-  const T* __restrict__ x = static_cast<const T*>(P.x);
   const int warp = int(threadIdx.x) >> 5, lane = int(threadIdx.x) & 31;
   const int nslices = (P.nrows + 31) >> 5;
   for (int tile = int(blockIdx.x) - P.block_begin; tile < P.ntiles;
@@ -151,8 +159,15 @@ __device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f) {
     const int g = P.row0 + slice * 32 + lane;  // global row (D16 base)
     T sum = T(0);
     for (int k0 = 0; k0 < w; k0 += U) {
+      // All U column and value loads first, then the U gathers, then the
+      // sums: each lane has 2U independent loads in flight, then U more.
+      // (The two index forms test padding differently: a 16-bit offset by
+      // its sentinel, a 32-bit column by its sign.  Both were measured
+      // against alternatives on the 7-point stencil; the compiler schedules
+      // the two forms best written this way.)
       T v[U];
       int c[U];
+      bool ok[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         if (k0 + u < w) {
@@ -160,37 +175,35 @@ __device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f) {
           if (D16) {
             const int16_t* offs = reinterpret_cast<const int16_t*>(cols);
             const int d = KEEP ? ld_pol(offs + idx, stream) : int(ld_stream(offs + idx));
-            c[u] = d == -32768 ? -1 : g + d;
+            ok[u] = d != -32768;
+            c[u] = g + d;
           } else {
             c[u] = KEEP ? ld_pol(cols + idx, stream) : ld_stream(cols + idx);
           }
           v[u] = KEEP ? ld_pol(vals + idx, stream) : ld_stream(vals + idx);
         } else {
           v[u] = T(0);
-          c[u] = -1;
+          c[u] = D16 ? 0 : -1;
+          ok[u] = false;
         }
+        if (!D16) ok[u] = c[u] >= 0;
       }
       T xv[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (KEEP)
-          xv[u] = c[u] >= 0 ? ld_pol(x + c[u], keep) : T(0);
-        else
-          xv[u] = c[u] >= 0 ? ld_gather(x + c[u]) : T(0);
-      }
+      for (int u = 0; u < U; ++u) xv[u] = ok[u] ? gx(P, c[u]) : T(0);
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        if (c[u] >= 0) sum += v[u] * xv[u];
+        if (ok[u]) sum += v[u] * xv[u];
     }
     const int row = slice * 32 + lane;
     if (row < P.nrows) f(P, row, sum);
   }
 }
 
-template <typename T, int BS, int U, bool D16 = false>
+template <typename T, int BS, int U, bool D16 = false, bool KEEP = false>
 __global__ void __launch_bounds__(BS)
     spmv_sell_kernel(const __grid_constant__ SpmvArgs a) {
-  sell_for_rows<T, BS, U, false, D16>(a, [](const PartArg& P, int row, T sum) {
+  sell_for_rows<T, BS, U, KEEP, D16>(a, [](const PartArg& P, int row, T sum) {
     static_cast<T*>(P.y)[row] = sum;
   });
 }

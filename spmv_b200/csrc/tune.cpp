@@ -2,11 +2,13 @@
 //
 // Candidates: vector CSR at half, equal and twice the statistics' lane count,
 // SELL-32 at 2..16 loads in flight per lane (when its padding is at most 2x
-// the nonzeros), and merge-path; each at 128, 256 and 512 threads per CTA.
+// the nonzeros), each at 128, 256 and 512 threads per CTA; the staged SELL-32
+// product at 4 and 8 gathers in flight per lane (its CTA shape is fixed); and
+// merge-path.
 // Every candidate runs once untimed (building any layout it needs), then
 // `reps` times between two CUDA events on the communicator's stream; the
-// fastest becomes the matrix's kernel, used by mult and by the solvers'
-// products.  With SPMV_B200_TUNE_CACHE naming a file, results are cached
+// fastest becomes the matrix's kernel for mult (the solvers time their own
+// products over the fused-halo layout).  With SPMV_B200_TUNE_CACHE naming a file, results are cached
 // there by matrix statistics (dtype, ranks, rows, nonzeros, longest row,
 // SELL padding) and a later matrix with the same statistics skips the timing.
 #include <cstdio>
@@ -74,6 +76,7 @@ void autotune(spmv_matrix A, int reps, spmv_tune_result* best) {
     A->kernel = r.kernel;
     A->width = r.width;
     A->block = r.block;
+    A->kernel_set = false;
     A->cg.reset();
     A->ir.reset();
     if (best) *best = r;
@@ -116,6 +119,12 @@ void autotune(spmv_matrix A, int reps, spmv_tune_result* best) {
     if (C.sell_padded <= 2 * std::max<int64_t>(nnz, 1))
       for (int u : {2, 4, 8, 16}) cands.push_back({SPMV_KERNEL_SELL, u, bs});
   }
+  {
+    int64_t nnz = 0;
+    for (const DevPart& D : C.parts) nnz += D.nnz;
+    if (C.sell_padded <= 2 * std::max<int64_t>(nnz, 1))
+      for (int u : {4, 8}) cands.push_back({SPMV_KERNEL_STAGED, u, 0});
+  }
   cands.push_back({SPMV_KERNEL_MERGE, 0, 256});
 
   cudaStream_t s = comm->stream;
@@ -125,7 +134,7 @@ void autotune(spmv_matrix A, int reps, spmv_tune_result* best) {
   double best_us = 1e300;
   Cand best_c = cands.front();
   for (const Cand& c : cands) {
-    if (c.k == SPMV_KERNEL_SELL) build_sell(A, A->fwd, s);
+    if (c.k == SPMV_KERNEL_SELL || c.k == SPMV_KERNEL_STAGED) build_sell(A, A->fwd, s);
     SpmvLaunch L{};
     L.csr = &A->fwd;
     L.cols = C.cols.as<int32_t>();
@@ -135,6 +144,7 @@ void autotune(spmv_matrix A, int reps, spmv_tune_result* best) {
     L.block = c.bs;
     L.num_sms = comm->num_sms;
     L.carry = &A->fwd.merge_carry;
+    L.err = comm->wait_flag();
     L.x = xs.data();
     L.y = ys.data();
     launch_spmv(L, s);
@@ -157,6 +167,7 @@ void autotune(spmv_matrix A, int reps, spmv_tune_result* best) {
   A->kernel = best_c.k;
   A->width = best_c.w;
   A->block = best_c.bs;
+  A->kernel_set = false;
   A->cg.reset();
   A->ir.reset();
   r.kernel = best_c.k;

@@ -20,7 +20,7 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--what", default="matvec", choices=["matvec", "cg"])
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
-    ap.add_argument("--kernel", default="auto", choices=["auto", "vector", "merge", "sell"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "vector", "merge", "sell", "staged"])
     args = ap.parse_args()
 
     import torch

@@ -199,6 +199,46 @@ def test_sell_is_bitwise_equal_to_oracle(cuda_device, cfg, P):
                                                        xs[q].astype(np.float32)))
 
 
+@pytest.mark.parametrize("cfg,P,width", [("c1", 1, 8), ("c2", 8, 4), ("c2", 3, 8), ("c3", 1, 8)])
+def test_staged_is_bitwise_equal_to_oracle(cuda_device, cfg, P, width):
+    # The staged SELL-32 product (tiles streamed into shared memory by bulk
+    # copies) also sums rows in storage order.
+    W = gen.workload(cfg, scale=0 if cfg != "c3" else 40)
+    comm, cm, rm, M, D = build(W, P)
+    M.set_kernel("staged", width)
+    assert M.get_kernel()[:2] == ("staged", width)
+    rng = np.random.default_rng(5)
+    xs = [rng.uniform(-1, 1, cm.vec_len(q)) for q in range(P)]
+    for _ in range(2):  # a second call reuses the tile table
+        ys = M.mult(xs)
+        for q in range(P):
+            rp, ci, va = D.blocks[q]
+            assert np.array_equal(ys[q], oracle.csr_mult(rp, ci, va, xs[q]))
+    comm.synchronize()  # no bounded wait timed out
+    M32 = S.Matrix(comm, [(rp, ci, va.astype(np.float32)) for rp, ci, va in D.blocks],
+                   cm, rm)
+    M32.set_kernel("staged", width)
+    ys32 = M32.mult([x.astype(np.float32) for x in xs])
+    for q in range(P):
+        rp, ci, va = D.blocks[q]
+        assert np.array_equal(ys32[q], oracle.csr_mult(rp, ci, va.astype(np.float32),
+                                                       xs[q].astype(np.float32)))
+
+
+def test_staged_wide_rows_fall_back(cuda_device):
+    # A slice wider than one stage cannot be staged: the product runs SELL-32
+    # from registers and still matches the oracle.
+    rng = np.random.default_rng(11)
+    A = random_csr(rng, 3000, 3000, density=0.002, long_rows=(3, 2900))
+    comm, cm, rm, M, D = build(A, 2)
+    M.set_kernel("staged", 8)
+    xs = [rng.standard_normal(cm.vec_len(q)) for q in range(2)]
+    ys = M.mult(xs)
+    for q in range(2):
+        rp, ci, va = D.blocks[q]
+        assert np.array_equal(ys[q], oracle.csr_mult(rp, ci, va, xs[q]))
+
+
 @pytest.mark.parametrize("width", [1, 2, 4, 8, 16])
 @pytest.mark.parametrize("block", [128, 256, 512])
 def test_sell_every_width_and_block(cuda_device, width, block):
@@ -231,5 +271,8 @@ def test_set_values_reaches_every_kernel_copy(cuda_device):
     assert np.array_equal(y, oracle.csr_mult(rp, ci, va * 4.0, xs[0]))
     x2, k2 = S.cg(comm, M, b, 10000, 1e-10)
     xm2, _ = S.cg_mixed(comm, M, b, 10000, 1e-10)
-    assert np.allclose(x2[0] * 4.0, x1[0], rtol=1e-7, atol=1e-12)
-    assert np.allclose(xm2[0] * 4.0, xm1[0], rtol=1e-7, atol=1e-12)
+    # Each solver workspace re-picks its product by timing after new values,
+    # so the two solves may sum rows in different orders: both solutions are
+    # within 1e-10 relative residual, close but not bitwise equal.
+    assert np.linalg.norm(x2[0] * 4.0 - x1[0]) <= 1e-6 * np.linalg.norm(x1[0])
+    assert np.linalg.norm(xm2[0] * 4.0 - xm1[0]) <= 1e-6 * np.linalg.norm(xm1[0])
