@@ -8,14 +8,18 @@
 //
 //   K1  y = A p and p.y           (SpMV with a dot-product epilogue; the last
 //                                  CTA forms alpha = rnorm_old / p.y)
-//   K2  x += alpha p, r -= alpha y, r.r
-//                                 (the last CTA forms beta, counts the
+//   K2  r -= alpha y, r.r         (the last CTA forms beta, counts the
 //                                  iteration, tests convergence and sets the
 //                                  graph's loop condition)
-//   K3  p = p beta + r
+//   K3  x += alpha p, p = p beta + r
+//                                 (x is updated where p is read anyway: 10
+//                                  vector passes per iteration instead of 11;
+//                                  the arithmetic is the reference's)
 //
 // The three kernels form the body of a CUDA-graph while node; an init kernel
-// before it sets r = p = b, x = 0 and rnorm0.  A whole solve is one graph
+// before it sets r = p = b, x = 0 and rnorm0.  (Programmatic dependent
+// launch of K2 and K3 was measured on the 7-point stencil and gained
+// nothing.)  A whole solve is one graph
 // launch with no host round trip per iteration.  Reductions are single pass
 // (per-CTA partials, the last CTA to arrive sums them in index order), so
 // results are reproducible run to run for a given product kernel.  Vector
@@ -160,10 +164,10 @@ __global__ void __launch_bounds__(SolverStaged::BS)
   });
 }
 
-// K2: x += alpha p, r -= alpha y, r.r; beta, the iteration count and the
-// convergence test.  Sets `h` to continue (1) or stop (0).
+// K2: r -= alpha y, r.r; beta, the iteration count and the convergence
+// test.  Sets `h` to continue (1) or stop (0).
 __global__ void __launch_bounds__(EW_BS)
-    cg_update_xr(const CgPtrs c, cudaGraphConditionalHandle h) {
+    cg_update_r(const CgPtrs c, cudaGraphConditionalHandle h) {
   __shared__ double smem[32];
   const bool ok = c.st->status == SPMV_SUCCESS;
   const double alpha = c.st->alpha;
@@ -172,7 +176,6 @@ __global__ void __launch_bounds__(EW_BS)
   if (ok) {
     for (int64_t i = blockIdx.x * int64_t(EW_BS) + threadIdx.x; i < c.n;
          i += int64_t(gridDim.x) * EW_BS) {
-      st_pol(c.x + i, ld_pol(c.x + i, keep) + alpha * ld_pol(c.p + i, keep), keep);
       const double ri = ld_pol(c.r + i, keep) - alpha * ld_pol(c.y + i, keep);
       st_pol(c.r + i, ri, keep);
       acc += ri * ri;
@@ -196,14 +199,19 @@ __global__ void __launch_bounds__(EW_BS)
   }
 }
 
-// K3: p = p beta + r.
-__global__ void __launch_bounds__(EW_BS) cg_update_p(const CgPtrs c) {
+// K3: x += alpha p, p = p beta + r (with this iteration's alpha and beta;
+// skipped, like K2's update, after a breakdown).
+__global__ void __launch_bounds__(EW_BS) cg_update_xp(const CgPtrs c) {
   if (c.st->status != SPMV_SUCCESS) return;
+  const double alpha = c.st->alpha;
   const double beta = c.st->beta;
   const uint64_t keep = l2_policy_keep();
   for (int64_t i = blockIdx.x * int64_t(EW_BS) + threadIdx.x; i < c.n;
-       i += int64_t(gridDim.x) * EW_BS)
-    st_pol(c.p + i, ld_pol(c.p + i, keep) * beta + ld_pol(c.r + i, keep), keep);
+       i += int64_t(gridDim.x) * EW_BS) {
+    const double pi = ld_pol(c.p + i, keep);
+    st_pol(c.x + i, ld_pol(c.x + i, keep) + alpha * pi, keep);
+    st_pol(c.p + i, pi * beta + ld_pol(c.r + i, keep), keep);
+  }
 }
 
 using K1Fn = void (*)(SpmvArgs, CgPtrs, cudaGraphConditionalHandle);
@@ -285,14 +293,15 @@ CgPtrs cg_ptrs(CgWorkspace& w) {
 
 void add_kernel(cudaGraphNode_t* node, cudaGraph_t g, const cudaGraphNode_t* dep,
                 size_t ndep, void* fn, int grid, int block, int smem, void** args) {
-  cudaKernelNodeParams kp{};
-  kp.func = fn;
-  kp.gridDim = dim3(grid);
-  kp.blockDim = dim3(block);
-  kp.sharedMemBytes = unsigned(smem);
-  kp.kernelParams = args;
-  kp.extra = nullptr;
-  SPMVB_CUDA(cudaGraphAddKernelNode(node, g, dep, ndep, &kp));
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeKernel;
+  np.kernel.func = fn;
+  np.kernel.gridDim = dim3(grid);
+  np.kernel.blockDim = dim3(block);
+  np.kernel.sharedMemBytes = unsigned(smem);
+  np.kernel.kernelParams = args;
+  np.kernel.extra = nullptr;
+  SPMVB_CUDA(cudaGraphAddNode(node, g, dep, ndep, &np));
 }
 
 // The staged tile table a product uses (FP64 values).
@@ -358,13 +367,13 @@ void build_graph(spmv_matrix A, CgWorkspace& w) {
   }
   {
     void* args[] = {&c, &w.h_loop};
-    add_kernel(&k2, body, k1 ? &k1 : nullptr, k1 ? 1 : 0, (void*)cg_update_xr, ew_grid, EW_BS,
+    add_kernel(&k2, body, k1 ? &k1 : nullptr, k1 ? 1 : 0, (void*)cg_update_r, ew_grid, EW_BS,
                0, args);
   }
   {
     cudaGraphNode_t k3;
     void* args[] = {&c};
-    add_kernel(&k3, body, &k2, 1, (void*)cg_update_p, ew_grid, EW_BS, 0, args);
+    add_kernel(&k3, body, &k2, 1, (void*)cg_update_xp, ew_grid, EW_BS, 0, args);
   }
   SPMVB_CUDA(cudaGraphInstantiate(&w.exec, w.graph, 0));
 }

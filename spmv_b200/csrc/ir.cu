@@ -162,7 +162,9 @@ __global__ void __launch_bounds__(kind_bs<KIND>())
   }
 }
 
-// K2: d += alpha p, r -= alpha y, r.r; decides whether to refine.
+// K2: r -= alpha y, r.r; decides whether to refine.  (The correction
+// update d += alpha p is made where p is read anyway: by K3, or by the fold
+// when this iteration refines.)
 __global__ void __launch_bounds__(EW)
     ir_update(const IrPtrs c, cudaGraphConditionalHandle h_ref) {
   __shared__ double smem[32];
@@ -172,7 +174,6 @@ __global__ void __launch_bounds__(EW)
   double acc = 0.0;
   if (ok) {
     IR_LOOP(i) {
-      st_pol(c.d + i, ld_pol(c.d + i, keep) + alpha * ld_pol(c.p + i, keep), keep);
       const float ri = ld_pol(c.r + i, keep) - alpha * ld_pol(c.y + i, keep);
       st_pol(c.r + i, ri, keep);
       acc += double(ri) * double(ri);
@@ -199,10 +200,13 @@ __global__ void __launch_bounds__(EW)
   }
 }
 
-// Refinement 1: fold the FP32 correction into the FP64 solution.
+// Refinement 1: fold the FP32 correction, with this iteration's alpha p,
+// into the FP64 solution.
 __global__ void __launch_bounds__(EW) ir_fold(const IrPtrs c) {
+  const float alpha = float(c.st->alpha);
   IR_LOOP(i) {
-    c.x[i] = c.x[i] + double(c.d[i]);
+    const float di = c.d[i] + alpha * c.p[i];
+    c.x[i] = c.x[i] + double(di);
     c.d[i] = 0.0f;
   }
 }
@@ -255,18 +259,23 @@ __global__ void __launch_bounds__(EW) ir_resync(const IrPtrs c) {
   }
 }
 
-// K3: p = r + beta (p - c r); sets the loop condition.
+// K3: d += alpha p (unless the fold did it), p = r + beta (p - c r); sets
+// the loop condition.
 __global__ void __launch_bounds__(EW)
     ir_update_p(const IrPtrs c, cudaGraphConditionalHandle h_loop) {
   const IrState* st = c.st;
   const bool stop = st->status != SPMV_SUCCESS || st->converged;
   if (!stop) {
+    const float alpha = float(st->alpha);
     const float beta = float(st->beta);
     const float cc = float(st->c);
+    const bool fold_d = st->refine == 0;
     const uint64_t keep = l2_policy_keep();
     IR_LOOP(i) {
       const float ri = ld_pol(c.r + i, keep);
-      st_pol(c.p + i, ri + beta * (ld_pol(c.p + i, keep) - cc * ri), keep);
+      const float pi = ld_pol(c.p + i, keep);
+      if (fold_d) st_pol(c.d + i, ld_pol(c.d + i, keep) + alpha * pi, keep);
+      st_pol(c.p + i, ri + beta * (pi - cc * ri), keep);
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
