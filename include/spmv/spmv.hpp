@@ -78,6 +78,8 @@ class L2GMap {
     detail::check(spmv_l2gmap_create(comm.handle(), local_size.data(), gp.data(),
                                      ng.data(), &h_));
   }
+  /// Takes ownership of a map handle (as returned by spmv_petsc_read_matrix).
+  explicit L2GMap(spmv_l2gmap adopted) : h_(adopted) {}
   ~L2GMap() { spmv_l2gmap_destroy(h_); }
   L2GMap(const L2GMap&) = delete;             // as L2GMap.h:36-37
   L2GMap& operator=(const L2GMap&) = delete;
@@ -184,6 +186,16 @@ class Matrix {
     nrows_ = nr;
     ncols_ = nc;
   }
+  /// Takes ownership of a matrix handle and its maps (as returned by
+  /// spmv_petsc_read_matrix) for a communicator of `size` ranks.
+  Matrix(spmv_matrix adopted, std::shared_ptr<L2GMap> col_map,
+         std::shared_ptr<L2GMap> row_map, int size)
+      : h_(adopted), col_map_(std::move(col_map)), row_map_(std::move(row_map)) {
+    for (int r = 0; r < size; ++r) {
+      nrows_.push_back(row_map_->local_size(r));
+      ncols_.push_back(col_map_->local_size(r) + col_map_->num_ghosts(r));
+    }
+  }
   ~Matrix() { spmv_matrix_destroy(h_); }
   // Move-only: the reference's implicit copy duplicates its MKL handle.
   Matrix(const Matrix&) = delete;
@@ -233,6 +245,36 @@ class Matrix {
   std::shared_ptr<L2GMap> col_map_, row_map_;
   std::vector<std::int32_t> nrows_, ncols_;
 };
+
+/// spmv::read_petsc_binary (read_petsc.h:18-24, read_petsc.cpp:32-191) for
+/// every rank: a PETSc binary matrix file split by owner_ranges.  Throws
+/// "Could not open file" and "Bad signature in PETSc Matrix file" as the
+/// reference does.
+inline Matrix<double> read_petsc_binary(const Comm& comm, const std::string& filename) {
+  spmv_l2gmap cm = nullptr, rm = nullptr;
+  spmv_matrix A = nullptr;
+  detail::check(spmv_petsc_read_matrix(comm.handle(), filename.c_str(), &cm, &rm, &A));
+  return Matrix<double>(A, std::make_shared<L2GMap>(cm), std::make_shared<L2GMap>(rm),
+                        comm.size());
+}
+
+/// spmv::read_petsc_binary_vector (read_petsc.h:26-32, read_petsc.cpp:193-260):
+/// every rank's owner_ranges block of a PETSc binary vector file.
+inline std::vector<std::vector<double>> read_petsc_binary_vector(const Comm& comm,
+                                                                 const std::string& filename) {
+  std::int64_t n = 0;
+  detail::check(spmv_petsc_vector_size(filename.c_str(), &n));
+  std::vector<std::int64_t> rr(size_t(comm.size()) + 1);
+  detail::check(spmv_owner_ranges(comm.size(), n, rr.data()));
+  std::vector<std::vector<double>> v(size_t(comm.size()));
+  std::vector<double*> vp(size_t(comm.size()));
+  for (int r = 0; r < comm.size(); ++r) {
+    v[r].resize(size_t(rr[r + 1] - rr[r]));
+    vp[r] = v[r].data();
+  }
+  detail::check(spmv_petsc_read_vector(comm.handle(), filename.c_str(), vp.data()));
+  return v;
+}
 
 /// spmv::cg (cg.h:27-29, cg.cpp:11-83) on every rank: returns x (each
 /// col_map local_size + num_ghosts long, ghost tail zero) and the iteration

@@ -369,6 +369,34 @@ int spmv_matrix_sample_outer(spmv_matrix A, spmv_memory memory, double scale,
                              const void* const* lambda, const void* const* x,
                              void* const* out);
 
+/* ------------------------------------------------------------------------ */
+/* PETSc binary files (reference: read_petsc.h:18-32, read_petsc.cpp)       */
+/* ------------------------------------------------------------------------ */
+
+/* owner_ranges (read_petsc.cpp:13-30, CreateA.cpp:12-29): ranges[size + 1]
+ * splitting n items over size ranks, the first n % size ranks one larger. */
+int spmv_owner_ranges(int size, int64_t n, int64_t* ranges);
+
+/* spmv::read_petsc_binary (read_petsc.cpp:32-191) for every rank of comm at
+ * once: a PETSc binary matrix file (32-bit indices, big endian) split by
+ * owner_ranges over rows and columns.  Rank r's columns are numbered owned
+ * first, then its ghosts in ascending global order; entries within a row are
+ * in ascending local column order.  Returns the FP64 matrix and its two maps
+ * (row map without ghosts); the caller destroys all three.  Errors: "Could
+ * not open file", "Bad signature in PETSc Matrix file", and (where the
+ * reference reads out of range) truncated files, row lengths that do not sum
+ * to nnz and column indices outside [0, ncols). */
+int spmv_petsc_read_matrix(spmv_comm comm, const char* filename, spmv_l2gmap* col_map,
+                           spmv_l2gmap* row_map, spmv_matrix* A);
+
+/* Length of a PETSc binary vector file ("Bad signature in PETSc Vector
+ * file" if it is not one). */
+int spmv_petsc_vector_size(const char* filename, int64_t* n);
+
+/* spmv::read_petsc_binary_vector (read_petsc.cpp:193-260) for every rank:
+ * values[r] (host) receives the rank's owner_ranges(size, n) block. */
+int spmv_petsc_read_vector(spmv_comm comm, const char* filename, double* const* values);
+
 #ifdef __cplusplus
 }
 #endif

@@ -56,6 +56,11 @@ def lib():
         L.oracle_matvec_demo.argtypes = [C.c_int, I64, C.c_int]
         L.oracle_matvec_demo.restype = D
         L.oracle_max_threads.restype = C.c_int
+        L.oracle_petsc_read.argtypes = [C.c_char_p, C.c_int]
+        L.oracle_petsc_read.restype = P
+        L.oracle_petsc_free.argtypes = [P]
+        L.oracle_petsc_block.argtypes = [P, C.c_int, C.c_int, C.POINTER(P)]
+        L.oracle_petsc_block.restype = I64
         _lib = L
     return _lib
 
@@ -160,3 +165,26 @@ def matvec_demo(P: int, N: int = 500000, n_apply: int = 1000) -> float:
 
 def max_threads() -> int:
     return lib().oracle_max_threads()
+
+
+def petsc_read(filename, P: int):
+    """read_petsc_binary restated (read_petsc.cpp:32-191) for P ranks:
+    per rank [rowptr, colind, values, ghosts]."""
+    L = lib()
+    h = L.oracle_petsc_read(str(filename).encode(), int(P))
+    if not h:
+        raise RuntimeError(L.oracle_last_error().decode())
+    try:
+        out = []
+        for r in range(P):
+            arrs = []
+            for field, ct, dt in ((0, C.c_int32, np.int32), (1, C.c_int32, np.int32),
+                                  (2, C.c_double, np.float64), (3, C.c_int64, np.int64)):
+                p = C.c_void_p()
+                n = L.oracle_petsc_block(h, r, field, C.byref(p))
+                arrs.append(np.ctypeslib.as_array(C.cast(p, C.POINTER(ct)), (n,)).copy()
+                            if n > 0 else np.zeros(0, dt))
+            out.append(arrs)
+        return out
+    finally:
+        L.oracle_petsc_free(h)

@@ -22,6 +22,8 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <fstream>
+#include <iterator>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -506,6 +508,125 @@ int oracle_max_threads(void) {
 #else
   return 1;
 #endif
+}
+
+// spmv::read_petsc_binary (read_petsc.cpp:32-191) restated for all P ranks:
+// big-endian header and arrays, rows and columns split by owner_ranges, the
+// rank's columns numbered through an ordered map (owned first, then the
+// other referenced columns in ascending order), entries inserted row by row
+// the way Eigen's SparseMatrix::insert places them (ascending inner index; a
+// repeated index goes after the ones already there) and then compressed.
+// Returns a handle to every rank's CSR and ghosts, or null with an error.
+typedef struct OraclePetsc* oracle_petsc;
+struct OraclePetsc {
+  struct Block {
+    std::vector<int32_t> rowptr, colind;
+    std::vector<double> vals;
+    std::vector<int64_t> ghosts;
+    int64_t ncols_local = 0;
+  };
+  std::vector<Block> blocks;
+};
+
+static int32_t swap_i32(const char* p) {
+  char b[4] = {p[3], p[2], p[1], p[0]};
+  int32_t v;
+  std::memcpy(&v, b, 4);
+  return v;
+}
+static double swap_f64(const char* p) {
+  char b[8] = {p[7], p[6], p[5], p[4], p[3], p[2], p[1], p[0]};
+  double v;
+  std::memcpy(&v, b, 8);
+  return v;
+}
+
+oracle_petsc oracle_petsc_read(const char* filename, int P) {
+  oracle_petsc h = nullptr;
+  const int st = guard([&] {
+    std::ifstream file(filename, std::ios::in | std::ios::binary);
+    if (!file.is_open()) throw std::runtime_error("Could not open file");
+    std::vector<char> all((std::istreambuf_iterator<char>(file)), std::istreambuf_iterator<char>());
+    if (all.size() < 16) throw std::runtime_error("short file");
+    if (swap_i32(&all[0]) != 1211216)
+      throw std::runtime_error("Bad signature in PETSc Matrix file");
+    const int64_t nrows = swap_i32(&all[4]), ncols = swap_i32(&all[8]),
+                  nnz_tot = swap_i32(&all[12]);
+    const size_t need = 16 + size_t(nrows) * 4 + size_t(nnz_tot) * 12;
+    if (all.size() < need) throw std::runtime_error("short file");
+    std::vector<int32_t> nnz(nrows);
+    for (int64_t i = 0; i < nrows; ++i) nnz[i] = swap_i32(&all[16 + 4 * i]);
+    const char* cols = &all[16 + 4 * nrows];
+    const char* vals = cols + 4 * nnz_tot;
+    std::vector<int64_t> row_ranges(P + 1), col_ranges(P + 1);
+    oracle_owner_ranges(P, nrows, row_ranges.data());
+    oracle_owner_ranges(P, ncols, col_ranges.data());
+    std::unique_ptr<OraclePetsc> out(new OraclePetsc);
+    out->blocks.resize(P);
+    for (int rank = 0; rank < P; ++rank) {
+      OraclePetsc::Block& B = out->blocks[rank];
+      int64_t nnz_offset = 0;
+      for (int64_t i = 0; i < row_ranges[rank]; ++i) nnz_offset += nnz[i];
+      std::map<int32_t, int32_t> col_indices;
+      int32_t c = 0;
+      for (int64_t col = col_ranges[rank]; col < col_ranges[rank + 1]; ++col)
+        col_indices.insert({int32_t(col), c++});
+      int64_t j = nnz_offset;
+      for (int64_t row = row_ranges[rank]; row < row_ranges[rank + 1]; ++row)
+        for (int32_t k = 0; k < nnz[row]; ++k, ++j)
+          col_indices.insert({swap_i32(cols + 4 * j), -1});
+      for (auto& q : col_indices)
+        if (q.second == -1) q.second = c++;
+      // Insert row by row into sorted inner vectors.
+      const int64_t m = row_ranges[rank + 1] - row_ranges[rank];
+      std::vector<std::vector<std::pair<int32_t, double>>> rows(m);
+      j = nnz_offset;
+      for (int64_t row = row_ranges[rank]; row < row_ranges[rank + 1]; ++row) {
+        auto& rv = rows[row - row_ranges[rank]];
+        for (int32_t k = 0; k < nnz[row]; ++k, ++j) {
+          const int32_t lc = col_indices[swap_i32(cols + 4 * j)];
+          const double v = swap_f64(vals + 8 * j);
+          // Eigen's insert: shift the larger inner indices up by one.
+          auto it = std::upper_bound(rv.begin(), rv.end(), lc,
+                                     [](int32_t a, const std::pair<int32_t, double>& e) {
+                                       return a < e.first;
+                                     });
+          rv.insert(it, {lc, v});
+        }
+      }
+      B.rowptr.push_back(0);
+      for (const auto& rv : rows) {
+        for (const auto& e : rv) {
+          B.colind.push_back(e.first);
+          B.vals.push_back(e.second);
+        }
+        B.rowptr.push_back(int32_t(B.colind.size()));
+      }
+      B.ncols_local = col_ranges[rank + 1] - col_ranges[rank];
+      B.ghosts.assign(col_indices.size() - B.ncols_local, 0);
+      for (auto& q : col_indices)
+        if (q.first < col_ranges[rank] || q.first >= col_ranges[rank + 1])
+          B.ghosts[q.second - B.ncols_local] = q.first;
+    }
+    h = out.release();
+  });
+  return st == 0 ? h : nullptr;
+}
+
+void oracle_petsc_free(oracle_petsc h) { delete h; }
+
+// Rank r's arrays: field 0 rowptr, 1 colind (int32); 2 values (double);
+// 3 ghosts (int64).  Returns the element count and the data pointer.
+int64_t oracle_petsc_block(oracle_petsc h, int rank, int field, const void** data) {
+  const OraclePetsc::Block& B = h->blocks[rank];
+  switch (field) {
+    case 0: *data = B.rowptr.data(); return int64_t(B.rowptr.size());
+    case 1: *data = B.colind.data(); return int64_t(B.colind.size());
+    case 2: *data = B.vals.data(); return int64_t(B.vals.size());
+    case 3: *data = B.ghosts.data(); return int64_t(B.ghosts.size());
+  }
+  *data = nullptr;
+  return -1;
 }
 
 }  // extern "C"

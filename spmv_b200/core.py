@@ -514,3 +514,46 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+# --------------------------------------------------------------------------
+# PETSc binary files and the owner_ranges split (read_petsc.cpp).
+# --------------------------------------------------------------------------
+
+def owner_ranges(size: int, n: int) -> List[int]:
+    """owner_ranges (read_petsc.cpp:13-30): size + 1 boundaries splitting n
+    items, the first n % size ranks one larger."""
+    r = (C.c_int64 * (int(size) + 1))()
+    call("spmv_owner_ranges", int(size), int(n), r)
+    return list(r)
+
+
+def read_petsc_binary(comm: Comm, filename: str) -> Matrix:
+    """spmv::read_petsc_binary (read_petsc.cpp:32-191) for every rank of
+    `comm`: the FP64 matrix of a PETSc binary file, rows and columns split by
+    owner_ranges; .col_map() / .row_map() are its maps."""
+    cm, rm, h = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    call("spmv_petsc_read_matrix", comm.handle, str(filename).encode(), C.byref(cm),
+         C.byref(rm), C.byref(h))
+    col_map = L2GMap.__new__(L2GMap)
+    col_map.comm, col_map._h = comm, cm
+    row_map = L2GMap.__new__(L2GMap)
+    row_map.comm, row_map._h = comm, rm
+    M = Matrix.__new__(Matrix)
+    M.comm, M._col_map, M._row_map, M._h = comm, col_map, row_map, h
+    M.np_dtype, M.dtype = np.dtype(np.float64), _lib.FLOAT64
+    M.nrows = [row_map.local_size(r) for r in range(comm.size)]
+    M.ncols = [col_map.vec_len(r) for r in range(comm.size)]
+    return M
+
+
+def read_petsc_binary_vector(comm: Comm, filename: str) -> List[np.ndarray]:
+    """spmv::read_petsc_binary_vector (read_petsc.cpp:193-260) for every
+    rank: rank r's owner_ranges block of a PETSc binary vector file."""
+    n = C.c_int64()
+    call("spmv_petsc_vector_size", str(filename).encode(), C.byref(n))
+    rr = owner_ranges(comm.size, n.value)
+    out = [np.empty(rr[q + 1] - rr[q], dtype=np.float64) for q in range(comm.size)]
+    call("spmv_petsc_read_vector", comm.handle, str(filename).encode(),
+         ptr_array([v.ctypes.data if len(v) else None for v in out]))
+    return out

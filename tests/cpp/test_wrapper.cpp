@@ -43,6 +43,30 @@ int main(int argc, char** argv) {
     EXPECT(m.global_offset(1) == 4 && m.global_to_local(0, 4) == 4);
     EXPECT(m.ghosts(1).size() == 1 && m.ghosts(1)[0] == 3);
   }
+  if (argc > 2) {
+    // argv[2]: a PETSc binary file of the 5x5 matrix with A[i][j] = 10 i + j
+    // on |i - j| <= 1, rows written with descending columns; argv[3] the
+    // vector 0..4.  Two ranks: rows/columns {0,1,2} and {3,4}.
+    spmv::Comm comm(2, -1);
+    spmv::Matrix<double> A = spmv::read_petsc_binary(comm, argv[2]);
+    EXPECT(A.rows(0) == 3 && A.rows(1) == 2);
+    EXPECT(A.col_map()->num_ghosts(0) == 1 && A.col_map()->ghosts(0)[0] == 3);
+    EXPECT(A.col_map()->num_ghosts(1) == 1 && A.col_map()->ghosts(1)[0] == 2);
+    const std::int32_t *rp = nullptr, *ci = nullptr;
+    const void* va = nullptr;
+    spmv::detail::check(spmv_matrix_csr(A.handle(), 1, &rp, &ci, &va));
+    // rank 1 row 0 (global 3): owned columns 3, 4 -> local 0, 1, then the
+    // ghost 2 -> local 2, in ascending local order.
+    const double* v = static_cast<const double*>(va);
+    EXPECT(rp[1] == 3 && ci[0] == 0 && ci[1] == 1 && ci[2] == 2);
+    EXPECT(v[0] == 33.0 && v[1] == 34.0 && v[2] == 32.0);
+    auto b = spmv::read_petsc_binary_vector(comm, argv[3]);
+    EXPECT(b.size() == 2 && b[0].size() == 3 && b[1].size() == 2 && b[1][1] == 4.0);
+    EXPECT(message_of([&] { spmv::read_petsc_binary(comm, argv[3]); }) ==
+           "Bad signature in PETSc Matrix file");
+    EXPECT(message_of([&] { spmv::read_petsc_binary(comm, "/nonexistent/x.dat"); }) ==
+           "Could not open file");
+  }
   if (gpu) {
     // 1D Laplacian [-1, 2, -1] on 12 points over 3 ranks of 4.
     const int P = 3, M = 4;

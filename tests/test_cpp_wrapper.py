@@ -20,8 +20,21 @@ def wrapper_exe(tmp_path_factory):
     return exe
 
 
-def test_cpp_wrapper_host(wrapper_exe):
-    r = subprocess.run([str(wrapper_exe), "host"], capture_output=True, text=True)
+def test_cpp_wrapper_host(wrapper_exe, tmp_path):
+    import numpy as np
+    from spmv_b200 import petsc
+    rp, ci, va = [0], [], []
+    for i in range(5):
+        for j in (i + 1, i, i - 1):  # descending columns in the file
+            if 0 <= j < 5:
+                ci.append(j)
+                va.append(10.0 * i + j)
+        rp.append(len(ci))
+    fa, fb = tmp_path / "A.dat", tmp_path / "b.dat"
+    petsc.write_matrix(fa, rp, ci, va, 5)
+    petsc.write_vector(fb, np.arange(5.0))
+    r = subprocess.run([str(wrapper_exe), "host", str(fa), str(fb)], capture_output=True,
+                       text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK 0 failures" in r.stdout
 
