@@ -13,6 +13,7 @@
 // Header-only; link with -lspmv_b200.
 #pragma once
 
+#include <complex>
 #include <cstdint>
 #include <memory>
 #include <stdexcept>
@@ -32,9 +33,14 @@ inline void check(int status) {
 }
 template <typename T>
 constexpr spmv_dtype dtype_of() {
-  static_assert(std::is_same<T, double>::value || std::is_same<T, float>::value,
-                "spmv_b200 matrices are float or double");
-  return std::is_same<T, double>::value ? SPMV_FLOAT64 : SPMV_FLOAT32;
+  static_assert(std::is_same<T, double>::value || std::is_same<T, float>::value ||
+                    std::is_same<T, std::complex<double>>::value ||
+                    std::is_same<T, std::complex<float>>::value,
+                "spmv_b200 scalars: float, double, std::complex<float>, std::complex<double>");
+  return std::is_same<T, double>::value                 ? SPMV_FLOAT64
+         : std::is_same<T, float>::value                ? SPMV_FLOAT32
+         : std::is_same<T, std::complex<double>>::value ? SPMV_COMPLEX128
+                                                        : SPMV_COMPLEX64;
 }
 }  // namespace detail
 

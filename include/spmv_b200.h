@@ -162,8 +162,13 @@ int spmv_l2gmap_reverse_update(spmv_l2gmap map, spmv_dtype dtype,
  * (Matrix.cpp:34-51): copies in every rank's local CSR block (0-based,
  * int32 row pointers and column indices, columns [0, ncols) with the
  * col_map's ghosts after its owned range).  nrows[size], ncols[size],
- * rowptr[size][nrows[r]+1], colind[size][nnz], values[size][nnz] of `dtype`.
- * row_map may be NULL (then rows have no map, and spmv_cg is refused). */
+ * rowptr[size][nrows[r]+1], colind[size][nnz], values[size][nnz] of `dtype`
+ * (float64, float32, complex128 or complex64 - the reference's four
+ * instantiations, Matrix.cpp:441-444; complex values interleaved re, im).
+ * row_map may be NULL (then rows have no map, and spmv_cg is refused).
+ * Complex matrices support mult and transpmult (plain transpose, result of
+ * ncols entries as in the generic path, Matrix.cpp:206-211); the solvers,
+ * SpMM and the adjoint sampling are real only. */
 int spmv_matrix_create_csr(spmv_comm comm, spmv_dtype dtype,
                            spmv_l2gmap col_map, spmv_l2gmap row_map,
                            const int32_t* nrows, const int32_t* ncols,

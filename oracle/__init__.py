@@ -50,6 +50,10 @@ def lib():
         L.oracle_csr_mult_f32.argtypes = [I32, P, P, P, P, P]
         L.oracle_csr_transpmult_f64.argtypes = [I32, I32, P, P, P, P, P]
         L.oracle_csr_transpmult_f32.argtypes = [I32, I32, P, P, P, P, P]
+        for n in ("oracle_csr_mult_c128", "oracle_csr_mult_c64"):
+            getattr(L, n).argtypes = [I32, P, P, P, P, P]
+        for n in ("oracle_csr_transpmult_c128", "oracle_csr_transpmult_c64"):
+            getattr(L, n).argtypes = [I32, I32, P, P, P, P, P]
         L.oracle_cg.argtypes = [P, C.c_int, P, P, P, P, P, P, C.c_int, D, C.c_int,
                                 C.c_int, C.POINTER(D)]
         L.oracle_cg.restype = C.c_int
@@ -121,22 +125,39 @@ class Map:
 
 
 def csr_mult(rp, ci, v, x, nthreads: int = 1) -> np.ndarray:
+    """Matrix::operator* restated (Eigen's row loop, storage order)."""
     m = len(rp) - 1
+    rp = np.ascontiguousarray(rp, np.int32)
+    ci = np.ascontiguousarray(ci, np.int32)
+    v = np.ascontiguousarray(v)
+    x = np.ascontiguousarray(x, v.dtype)
     y = np.empty(m, v.dtype)
+    args = (m, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, x.ctypes.data, y.ctypes.data)
     if v.dtype == np.float64:
-        lib().oracle_csr_mult_f64(m, rp.ctypes.data, ci.ctypes.data, v.ctypes.data,
-                                  x.ctypes.data, y.ctypes.data, nthreads)
+        lib().oracle_csr_mult_f64(*args, nthreads)
+    elif v.dtype == np.float32:
+        lib().oracle_csr_mult_f32(*args)
+    elif v.dtype == np.complex128:
+        lib().oracle_csr_mult_c128(*args)
+    elif v.dtype == np.complex64:
+        lib().oracle_csr_mult_c64(*args)
     else:
-        lib().oracle_csr_mult_f32(m, rp.ctypes.data, ci.ctypes.data, v.ctypes.data,
-                                  x.ctypes.data, y.ctypes.data)
+        raise TypeError(v.dtype)
     return y
 
 
 def csr_transpmult(rp, ci, v, x, ncols: int) -> np.ndarray:
+    """Matrix::transpmult restated (column scatter, no conjugation)."""
     m = len(rp) - 1
+    rp = np.ascontiguousarray(rp, np.int32)
+    ci = np.ascontiguousarray(ci, np.int32)
+    v = np.ascontiguousarray(v)
+    x = np.ascontiguousarray(x, v.dtype)
     y = np.empty(ncols, v.dtype)
-    f = (lib().oracle_csr_transpmult_f64 if v.dtype == np.float64
-         else lib().oracle_csr_transpmult_f32)
+    f = {np.dtype(np.float64): lib().oracle_csr_transpmult_f64,
+         np.dtype(np.float32): lib().oracle_csr_transpmult_f32,
+         np.dtype(np.complex128): lib().oracle_csr_transpmult_c128,
+         np.dtype(np.complex64): lib().oracle_csr_transpmult_c64}[v.dtype]
     f(m, ncols, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, x.ctypes.data,
       y.ctypes.data)
     return y

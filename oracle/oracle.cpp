@@ -20,6 +20,7 @@
 // and sums round separately, as they do there.
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <cstring>
 #include <fstream>
@@ -349,6 +350,33 @@ void oracle_csr_transpmult_f32(int32_t m, int32_t n, const int32_t* rp,
                                const int32_t* ci, const float* v,
                                const float* x, float* y) {
   csr_transpmult<float>(m, n, rp, ci, v, x, y);
+}
+// Complex instantiations (Matrix.cpp:441-444; the generic Eigen products of
+// Matrix.cpp:199-211, std::complex arithmetic).  Arrays are interleaved
+// (re, im) pairs.
+void oracle_csr_mult_c128(int32_t m, const int32_t* rp, const int32_t* ci, const void* v,
+                          const void* x, void* y) {
+  using C = std::complex<double>;
+  csr_mult<C>(m, rp, ci, static_cast<const C*>(v), static_cast<const C*>(x),
+              static_cast<C*>(y), 1);
+}
+void oracle_csr_mult_c64(int32_t m, const int32_t* rp, const int32_t* ci, const void* v,
+                         const void* x, void* y) {
+  using C = std::complex<float>;
+  csr_mult<C>(m, rp, ci, static_cast<const C*>(v), static_cast<const C*>(x),
+              static_cast<C*>(y), 1);
+}
+void oracle_csr_transpmult_c128(int32_t m, int32_t n, const int32_t* rp, const int32_t* ci,
+                                const void* v, const void* x, void* y) {
+  using C = std::complex<double>;
+  csr_transpmult<C>(m, n, rp, ci, static_cast<const C*>(v), static_cast<const C*>(x),
+                    static_cast<C*>(y));
+}
+void oracle_csr_transpmult_c64(int32_t m, int32_t n, const int32_t* rp, const int32_t* ci,
+                               const void* v, const void* x, void* y) {
+  using C = std::complex<float>;
+  csr_transpmult<C>(m, n, rp, ci, static_cast<const C*>(v), static_cast<const C*>(x),
+                    static_cast<C*>(y));
 }
 
 // spmv::cg (cg.cpp:11-83) on all ranks.  The row map is assumed ghost-free

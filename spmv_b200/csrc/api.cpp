@@ -213,6 +213,9 @@ void build_transpose(spmv_matrix A) {
   T.nz_total = nzo + 4;
   T.mean_row = rows > 0 ? double(nnz_all) / double(rows) : 0.0;
   T.max_row = maxr;
+  T.sell_padded = 0;
+  for (int r = 0; r < P; ++r)
+    T.sell_padded += sell_padded_size(rp[r], T.parts[r].nrows, nullptr);
   DeviceGuard dg(A->comm->device);
   T.rowptr.reserve(sizeof(int32_t) * std::max<int64_t>(T.rp_total, 1));
   T.cols.reserve(sizeof(int32_t) * T.nz_total);
@@ -229,6 +232,7 @@ void build_transpose(spmv_matrix A) {
     SPMVB_CUDA(cudaMemcpy(T.vals.as<char>() + D.nz_off * es, va[r].data(),
                           es * D.nnz, cudaMemcpyHostToDevice));
   }
+  A->h_trn_rowptr = std::move(rp);
   A->trn_built = true;
 }
 
@@ -267,9 +271,13 @@ void product(spmv_matrix A, bool transpose, spmv_memory memory,
           "spmv: unknown memory kind");
   DeviceGuard dg(comm->device);
   if (transpose) build_transpose(A);
-  const spmv_kernel picked = pick_kernel(A->kernel, A->fwd);
-  if (!transpose && (picked == SPMV_KERNEL_SELL || picked == SPMV_KERNEL_STAGED))
-    build_sell(A, A->fwd, comm->stream);
+  // The transpose's kernel follows its own row statistics (a kernel set on
+  // the matrix is for the forward product); SELL-32 sums each row of A^T in
+  // ascending row order of A, the reference's column-scatter order.
+  const spmv_kernel requested = transpose ? SPMV_KERNEL_AUTO : A->kernel;
+  const spmv_kernel picked = pick_kernel(requested, transpose ? A->trn : A->fwd);
+  if (picked == SPMV_KERNEL_SELL || picked == SPMV_KERNEL_STAGED)
+    build_sell(A, transpose ? A->trn : A->fwd, comm->stream);
   const DevCsr& C = transpose ? A->trn : A->fwd;
   const int P = comm->size;
   const size_t es = dtype_size(A->dtype);
@@ -282,9 +290,9 @@ void product(spmv_matrix A, bool transpose, spmv_memory memory,
   L.csr = &C;
   L.cols = C.cols.as<int32_t>();
   L.dtype = A->dtype;
-  L.kernel = A->kernel;
+  L.kernel = requested;
   L.width = transpose ? 0 : A->width;
-  L.block = A->block;
+  L.block = transpose ? 0 : A->block;
   L.num_sms = comm->num_sms;
   L.carry = transpose ? &A->trn.merge_carry : &A->fwd.merge_carry;
   L.err = comm->wait_flag();
@@ -651,8 +659,9 @@ int spmv_matrix_create_csr(spmv_comm comm, spmv_dtype dtype,
     check_comm(comm);
     require(out != nullptr, "spmv: NULL output");
     *out = nullptr;
-    require(dtype == SPMV_FLOAT64 || dtype == SPMV_FLOAT32,
-            "spmv::Matrix - Error: only float64 and float32 matrices are implemented");
+    require(dtype == SPMV_FLOAT64 || dtype == SPMV_FLOAT32 || dtype == SPMV_COMPLEX64 ||
+                dtype == SPMV_COMPLEX128,
+            "spmv::Matrix - Error: unknown dtype");
     require(nrows && ncols && rowptr && colind && values,
             "spmv::Matrix - Error: NULL CSR array");
     require(!col_map || col_map->comm == comm,

@@ -265,6 +265,7 @@ struct spmv_matrix_s {
   spmvb::DevCsr fwd;            // A
   spmvb::DevCsr trn;            // A^T, built on first transpmult
   bool trn_built = false;
+  std::vector<std::vector<int32_t>> h_trn_rowptr;  // A^T's row pointers (SELL build)
   // Kernel choice.
   spmv_kernel kernel = SPMV_KERNEL_AUTO;
   int width = 0, block = 0;

@@ -66,15 +66,94 @@ __device__ __forceinline__ int comp(const int4& v, int i) {
   return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
 }
 
+// Complex scalar with the layout of std::complex<F> (re, im).  The product
+// rounds as std::complex's does for finite values without FMA contraction:
+// re = a.re b.re - a.im b.im, im = a.re b.im + a.im b.re, each product and
+// sum rounded separately (the library is compiled with -fmad=false).
+template <typename F>
+struct alignas(2 * sizeof(F)) Cplx {
+  F re, im;
+  Cplx() = default;
+  __host__ __device__ constexpr Cplx(F r, F i = F(0)) : re(r), im(i) {}
+};
+template <typename F>
+__device__ __forceinline__ Cplx<F> operator*(const Cplx<F>& a, const Cplx<F>& b) {
+  return Cplx<F>(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+template <typename F>
+__device__ __forceinline__ Cplx<F> operator+(const Cplx<F>& a, const Cplx<F>& b) {
+  return Cplx<F>(a.re + b.re, a.im + b.im);
+}
+template <typename F>
+__device__ __forceinline__ Cplx<F>& operator+=(Cplx<F>& a, const Cplx<F>& b) {
+  a.re += b.re;
+  a.im += b.im;
+  return a;
+}
+using c64 = Cplx<float>;
+using c128 = Cplx<double>;
+
 // Streaming loads for matrix data (read once per product): evict-first.
 template <typename V>
 __device__ __forceinline__ V ld_stream(const V* p) {
   return __ldcs(p);
 }
+__device__ __forceinline__ c128 ld_stream(const c128* p) {
+  const double2 v = __ldcs(reinterpret_cast<const double2*>(p));
+  return c128(v.x, v.y);
+}
+__device__ __forceinline__ c64 ld_stream(const c64* p) {
+  const float2 v = __ldcs(reinterpret_cast<const float2*>(p));
+  return c64(v.x, v.y);
+}
 // Read-only cached load for gathered vector entries.
 template <typename T>
 __device__ __forceinline__ T ld_gather(const T* p) {
   return __ldg(p);
+}
+__device__ __forceinline__ c128 ld_gather(const c128* p) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  return c128(v.x, v.y);
+}
+__device__ __forceinline__ c64 ld_gather(const c64* p) {
+  const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+  return c64(v.x, v.y);
+}
+
+// Vector widths of the vector-CSR loads for complex values: one complex
+// double or two complex floats per 16-byte load.
+struct alignas(16) c64x2 {
+  c64 a, b;
+};
+__device__ __forceinline__ c64x2 ld_stream(const c64x2* p) {
+  const float4 v = __ldcs(reinterpret_cast<const float4*>(p));
+  return c64x2{c64(v.x, v.y), c64(v.z, v.w)};
+}
+template <>
+struct VecT<c128> {
+  static constexpr int N = 1;
+  using V = c128;
+  using C = int;
+};
+template <>
+struct VecT<c64> {
+  static constexpr int N = 2;
+  using V = c64x2;
+  using C = int2;
+};
+__device__ __forceinline__ c128 comp(const c128& v, int) { return v; }
+__device__ __forceinline__ int comp(int v, int) { return v; }
+__device__ __forceinline__ c64 comp(const c64x2& v, int i) { return i == 0 ? v.a : v.b; }
+
+// Butterfly shuffle within groups of W lanes (real and complex).
+template <typename T>
+__device__ __forceinline__ T shfl_xor(T v, int o, int W) {
+  return __shfl_xor_sync(0xffffffffu, v, o, W);
+}
+template <typename F>
+__device__ __forceinline__ Cplx<F> shfl_xor(Cplx<F> v, int o, int W) {
+  return Cplx<F>(__shfl_xor_sync(0xffffffffu, v.re, o, W),
+                 __shfl_xor_sync(0xffffffffu, v.im, o, W));
 }
 
 // L2 cache policies (per-instruction hints; no device setting is touched).

@@ -58,28 +58,31 @@ __global__ void sell_to_float(const double* __restrict__ in, float* __restrict__
 }
 
 // Scatters every rank's CSR (cols_in, optional vals_in) into SELL arrays.
-template <typename CI>
-void scatter_all(spmv_matrix A, DevCsr& C, const CI* cols_in, CI* cols_out,
-                 bool with_vals, CI pad, cudaStream_t s) {
-  const int grid = std::max(1, A->comm->num_sms) * 8;
+template <typename T, typename CI>
+void scatter_t(DevCsr& C, const CI* cols_in, CI* cols_out, bool with_vals, CI pad, int grid,
+               cudaStream_t s) {
   for (size_t r = 0; r < C.parts.size(); ++r) {
     const DevPart& D = C.parts[r];
     const int nslices = (D.nrows + 31) / 32;
     if (nslices == 0) continue;
     const int32_t* rp = C.rowptr.as<int32_t>() + D.rp_off;
     const int32_t* so = C.sell_off.as<int32_t>() + D.sl_off;
-    if (A->dtype == SPMV_FLOAT64) {
-      csr_to_sell<double, CI><<<grid, 256, 0, s>>>(
-          rp, cols_in + D.nz_off, C.vals.as<double>() + D.nz_off, so, D.nrows, nslices,
-          cols_out + D.sz_off, with_vals ? C.sell_vals.as<double>() + D.sz_off : nullptr,
-          pad);
-    } else {
-      csr_to_sell<float, CI><<<grid, 256, 0, s>>>(
-          rp, cols_in + D.nz_off, C.vals.as<float>() + D.nz_off, so, D.nrows, nslices,
-          cols_out + D.sz_off, with_vals ? C.sell_vals.as<float>() + D.sz_off : nullptr,
-          pad);
-    }
+    csr_to_sell<T, CI><<<grid, 256, 0, s>>>(
+        rp, cols_in + D.nz_off, C.vals.as<T>() + D.nz_off, so, D.nrows, nslices,
+        cols_out + D.sz_off, with_vals ? C.sell_vals.as<T>() + D.sz_off : nullptr, pad);
     SPMVB_CUDA(cudaGetLastError());
+  }
+}
+
+template <typename CI>
+void scatter_all(spmv_matrix A, DevCsr& C, const CI* cols_in, CI* cols_out,
+                 bool with_vals, CI pad, cudaStream_t s) {
+  const int grid = std::max(1, A->comm->num_sms) * 8;
+  switch (A->dtype) {
+    case SPMV_FLOAT64: scatter_t<double>(C, cols_in, cols_out, with_vals, pad, grid, s); break;
+    case SPMV_FLOAT32: scatter_t<float>(C, cols_in, cols_out, with_vals, pad, grid, s); break;
+    case SPMV_COMPLEX128: scatter_t<c128>(C, cols_in, cols_out, with_vals, pad, grid, s); break;
+    case SPMV_COMPLEX64: scatter_t<c64>(C, cols_in, cols_out, with_vals, pad, grid, s); break;
   }
 }
 
@@ -103,7 +106,9 @@ int64_t sell_padded_size(const std::vector<int32_t>& rowptr, int32_t nrows,
 
 void build_sell(spmv_matrix A, DevCsr& C, cudaStream_t stream) {
   if (C.sell_built) return;
-  require(&C == &A->fwd, "spmv: SELL layout is built for the forward matrix only");
+  require(&C == &A->fwd || (&C == &A->trn && A->trn_built),
+          "spmv: SELL layout of an unknown matrix copy");
+  const auto& h_rowptr = &C == &A->fwd ? A->h_rowptr : A->h_trn_rowptr;
   const int P = A->comm->size;
   const size_t es = dtype_size(A->dtype);
   std::vector<int32_t> all_off;
@@ -111,7 +116,7 @@ void build_sell(spmv_matrix A, DevCsr& C, cudaStream_t stream) {
   for (int r = 0; r < P; ++r) {
     DevPart& D = C.parts[r];
     std::vector<int32_t> soff;
-    const int64_t padded = sell_padded_size(A->h_rowptr[r], D.nrows, &soff);
+    const int64_t padded = sell_padded_size(h_rowptr[r], D.nrows, &soff);
     require(padded < (int64_t(1) << 31), "spmv: rank too large for 32-bit SELL offsets");
     D.sl_off = int64_t(all_off.size());
     D.sz_off = sz;
@@ -322,18 +327,19 @@ void launch_sell(const SpmvLaunch& L, const int32_t* sell_cols, cudaStream_t str
   fill_sell_args(a, C, sell_cols, C.sell_vals.ptr, es, L.x, L.y, nullptr, BS,
                  max_blocks_for(L.num_sms, BS));
   if (a.nblocks == 0) return;
-  if (L.dtype == SPMV_FLOAT64) {
+  auto by_bs = [&](auto tag) {
+    using T = decltype(tag);
     switch (BS) {
-      case 128: launch_sell_u<double, 128>(a, U, stream); break;
-      case 256: launch_sell_u<double, 256>(a, U, stream); break;
-      case 512: launch_sell_u<double, 512>(a, U, stream); break;
+      case 128: launch_sell_u<T, 128>(a, U, stream); break;
+      case 256: launch_sell_u<T, 256>(a, U, stream); break;
+      case 512: launch_sell_u<T, 512>(a, U, stream); break;
     }
-  } else {
-    switch (BS) {
-      case 128: launch_sell_u<float, 128>(a, U, stream); break;
-      case 256: launch_sell_u<float, 256>(a, U, stream); break;
-      case 512: launch_sell_u<float, 512>(a, U, stream); break;
-    }
+  };
+  switch (L.dtype) {
+    case SPMV_FLOAT64: by_bs(double{}); break;
+    case SPMV_FLOAT32: by_bs(float{}); break;
+    case SPMV_COMPLEX128: by_bs(c128{}); break;
+    case SPMV_COMPLEX64: by_bs(c64{}); break;
   }
   SPMVB_CUDA(cudaGetLastError());
 }

@@ -20,7 +20,8 @@
 namespace spmvb {
 
 int auto_width(double mean_row, spmv_dtype dtype) {
-  const int N = dtype == SPMV_FLOAT32 ? 4 : 2;
+  // Entries per 16-byte load.
+  const int N = dtype == SPMV_FLOAT32 ? 4 : (dtype == SPMV_COMPLEX128 ? 1 : 2);
   // Slots one pass must cover: the row plus up to N-1 entries of the
   // alignment head.
   const double slots = mean_row + (N - 1);
@@ -247,15 +248,18 @@ int max_blocks_for(int num_sms, int BS) {
 }
 
 void launch_spmv(const SpmvLaunch& L, cudaStream_t stream) {
-  require(L.dtype == SPMV_FLOAT64 || L.dtype == SPMV_FLOAT32,
-          "spmv: only float64 and float32 products are implemented");
+  const bool cplx = L.dtype == SPMV_COMPLEX64 || L.dtype == SPMV_COMPLEX128;
   const int W = L.width > 0 ? L.width : auto_width(L.csr->mean_row, L.dtype);
   const int BS = L.block > 0 ? L.block : 256;
   require(W >= 1 && W <= 32 && (W & (W - 1)) == 0,
           "spmv: width must be 1..32, a power of two");
   require(BS == 128 || BS == 256 || BS == 512,
           "spmv: block must be 128, 256 or 512");
-  const spmv_kernel k = pick_kernel(L.kernel, *L.csr, L.csr->sell_built);
+  spmv_kernel k = pick_kernel(L.kernel, *L.csr, L.csr->sell_built);
+  // Complex products run SELL-32 or vector CSR (merge-path and the staged
+  // pipeline are real only).
+  if (cplx && k == SPMV_KERNEL_MERGE) k = SPMV_KERNEL_VECTOR;
+  if (cplx && k == SPMV_KERNEL_STAGED) k = SPMV_KERNEL_SELL;
   if (k == SPMV_KERNEL_MERGE) {
     require(L.carry != nullptr, "spmv: merge-path product needs a carry buffer");
     launch_merge(L, stream, *L.carry);
@@ -274,10 +278,12 @@ void launch_spmv(const SpmvLaunch& L, cudaStream_t stream) {
   fill_spmv_args(a, *L.csr, L.cols, es, L.x, L.y, nullptr, BS / W,
                  max_blocks_for(L.num_sms, BS));
   if (a.nblocks == 0) return;
-  if (L.dtype == SPMV_FLOAT64)
-    launch_vector_bs<double>(a, W, BS, stream);
-  else
-    launch_vector_bs<float>(a, W, BS, stream);
+  switch (L.dtype) {
+    case SPMV_FLOAT64: launch_vector_bs<double>(a, W, BS, stream); break;
+    case SPMV_FLOAT32: launch_vector_bs<float>(a, W, BS, stream); break;
+    case SPMV_COMPLEX128: launch_vector_bs<c128>(a, W, BS, stream); break;
+    case SPMV_COMPLEX64: launch_vector_bs<c64>(a, W, BS, stream); break;
+  }
   SPMVB_CUDA(cudaGetLastError());
 }
 

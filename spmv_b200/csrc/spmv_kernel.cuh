@@ -24,7 +24,10 @@ struct XGather {
   __device__ __forceinline__ XGather() : pol(KEEP ? l2_policy_keep() : 0) {}
   __device__ __forceinline__ T operator()(const PartArg& P, int c) const {
     const T* x = static_cast<const T*>(P.x);
-    return KEEP ? ld_pol(x + c, pol) : ld_gather(x + c);
+    if constexpr (KEEP)
+      return ld_pol(x + c, pol);
+    else
+      return ld_gather(x + c);
   }
 };
 
@@ -49,8 +52,7 @@ __device__ __forceinline__ T row_dot(const int32_t* __restrict__ cols,
     }
   }
 #pragma unroll
-  for (int o = W / 2; o > 0; o >>= 1)
-    sum += __shfl_xor_sync(0xffffffffu, sum, o, W);
+  for (int o = W / 2; o > 0; o >>= 1) sum += shfl_xor(sum, o, W);
   return sum;
 }
 
@@ -92,8 +94,7 @@ __device__ __forceinline__ T row_dot16(const int16_t* __restrict__ offs,
     }
   }
 #pragma unroll
-  for (int o = W / 2; o > 0; o >>= 1)
-    sum += __shfl_xor_sync(0xffffffffu, sum, o, W);
+  for (int o = W / 2; o > 0; o >>= 1) sum += shfl_xor(sum, o, W);
   return sum;
 }
 
@@ -116,7 +117,7 @@ __device__ __forceinline__ void for_rows(const SpmvArgs& a, F&& f, const G& gx =
       e = __ldg(P.rowptr + row + 1);
     }
     T sum;
-    if (D16)
+    if constexpr (D16)
       sum = row_dot16<T, W>(reinterpret_cast<const int16_t*>(cols), vals, P, gx,
                             P.row0 + row, s, e, lane);
     else
@@ -180,7 +181,10 @@ __device__ __forceinline__ void sell_for_rows(const SpmvArgs& a, F&& f, const G&
           } else {
             c[u] = KEEP ? ld_pol(cols + idx, stream) : ld_stream(cols + idx);
           }
-          v[u] = KEEP ? ld_pol(vals + idx, stream) : ld_stream(vals + idx);
+          if constexpr (KEEP)
+            v[u] = ld_pol(vals + idx, stream);
+          else
+            v[u] = ld_stream(vals + idx);
         } else {
           v[u] = T(0);
           c[u] = D16 ? 0 : -1;

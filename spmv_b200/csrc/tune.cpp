@@ -119,13 +119,15 @@ void autotune(spmv_matrix A, int reps, spmv_tune_result* best) {
     if (C.sell_padded <= 2 * std::max<int64_t>(nnz, 1))
       for (int u : {2, 4, 8, 16}) cands.push_back({SPMV_KERNEL_SELL, u, bs});
   }
-  {
+  // Staged and merge-path products are real only.
+  const bool cplx = A->dtype == SPMV_COMPLEX64 || A->dtype == SPMV_COMPLEX128;
+  if (!cplx) {
     int64_t nnz = 0;
     for (const DevPart& D : C.parts) nnz += D.nnz;
     if (C.sell_padded <= 2 * std::max<int64_t>(nnz, 1))
       for (int u : {4, 8}) cands.push_back({SPMV_KERNEL_STAGED, u, 0});
+    cands.push_back({SPMV_KERNEL_MERGE, 0, 256});
   }
-  cands.push_back({SPMV_KERNEL_MERGE, 0, 256});
 
   cudaStream_t s = comm->stream;
   cudaEvent_t e0, e1;
