@@ -203,6 +203,42 @@ class Matrix {
     }
   }
   ~Matrix() { spmv_matrix_destroy(h_); }
+
+  /// Matrix::create_matrix (Matrix.cpp:213-438) for every rank: blocks[r]
+  /// holds nrows_local[r] owned rows then one row per row_ghosts[r] entry,
+  /// columns owned first then col_ghosts[r]; ghost rows are summed into
+  /// their owners and the column maps grow by the columns they bring.
+  static Matrix create_matrix(const Comm& comm, const std::vector<CsrBlock<T>>& blocks,
+                              const std::vector<std::int64_t>& nrows_local,
+                              const std::vector<std::int64_t>& ncols_local,
+                              const std::vector<std::vector<std::int64_t>>& row_ghosts,
+                              const std::vector<std::vector<std::int64_t>>& col_ghosts) {
+    const int P = comm.size();
+    if (int(blocks.size()) != P || int(nrows_local.size()) != P ||
+        int(ncols_local.size()) != P || int(row_ghosts.size()) != P ||
+        int(col_ghosts.size()) != P)
+      throw std::runtime_error("spmv::Matrix::create_matrix - Error: need one entry per rank");
+    std::vector<const std::int32_t*> rp(P), ci(P);
+    std::vector<const void*> va(P);
+    std::vector<const std::int64_t*> rg(P), cg(P);
+    std::vector<std::int64_t> nrg(P), ncg(P);
+    for (int r = 0; r < P; ++r) {
+      rp[r] = blocks[r].rowptr.data();
+      ci[r] = blocks[r].colind.data();
+      va[r] = blocks[r].values.data();
+      rg[r] = row_ghosts[r].data();
+      cg[r] = col_ghosts[r].data();
+      nrg[r] = std::int64_t(row_ghosts[r].size());
+      ncg[r] = std::int64_t(col_ghosts[r].size());
+    }
+    spmv_l2gmap cm = nullptr, rm = nullptr;
+    spmv_matrix A = nullptr;
+    detail::check(spmv_matrix_create_assembled(
+        comm.handle(), detail::dtype_of<T>(), nrows_local.data(), ncols_local.data(), rp.data(),
+        ci.data(), va.data(), rg.data(), nrg.data(), cg.data(), ncg.data(), &cm, &rm, &A));
+    return Matrix(A, std::make_shared<L2GMap>(cm), std::make_shared<L2GMap>(rm), P);
+  }
+
   // Move-only: the reference's implicit copy duplicates its MKL handle.
   Matrix(const Matrix&) = delete;
   Matrix& operator=(const Matrix&) = delete;

@@ -176,6 +176,25 @@ int spmv_matrix_create_csr(spmv_comm comm, spmv_dtype dtype,
                            const int32_t* const* colind,
                            const void* const* values, spmv_matrix* A);
 int spmv_matrix_destroy(spmv_matrix A);
+/* Matrix::create_matrix (Matrix.cpp:213-438) for every rank: rank r's block
+ * has nrows_local[r] owned rows followed by n_row_ghosts[r] ghost rows
+ * (global indices row_ghosts[r][i], rows other ranks own), and columns
+ * numbered owned first (ncols_local[r]) then col_ghosts[r] (sorted global
+ * indices); rowptr[r] has nrows_local[r] + n_row_ghosts[r] + 1 entries.
+ * Ghost rows are added into their owners' rows (entries with the same row
+ * and column summed in the reference's triplet order: the owner's rows
+ * first, then received rows by ascending sender), the owners' ghost columns
+ * grow by the columns those rows bring (ascending), and each row ends in
+ * ascending column order.  Returns the assembled matrix and its two maps
+ * (row map without ghosts); the caller destroys all three.  Ranges are the
+ * prefix sums of nrows_local and ncols_local. */
+int spmv_matrix_create_assembled(spmv_comm comm, spmv_dtype dtype, const int64_t* nrows_local,
+                                 const int64_t* ncols_local, const int32_t* const* rowptr,
+                                 const int32_t* const* colind, const void* const* values,
+                                 const int64_t* const* row_ghosts, const int64_t* n_row_ghosts,
+                                 const int64_t* const* col_ghosts,
+                                 const int64_t* n_col_ghosts, spmv_l2gmap* col_map,
+                                 spmv_l2gmap* row_map, spmv_matrix* A);
 /* Matrix::operator* (Matrix.cpp:158-166, 199-204): y[r] = A[r] x[r] for all
  * ranks in one launch.  x[r] has ncols[r] entries (owned, then ghosts: run
  * spmv_l2gmap_update first, as the reference's callers do), y[r] nrows[r]. */

@@ -65,6 +65,11 @@ def lib():
         L.oracle_petsc_free.argtypes = [P]
         L.oracle_petsc_block.argtypes = [P, C.c_int, C.c_int, C.POINTER(P)]
         L.oracle_petsc_block.restype = I64
+        L.oracle_create_matrix.argtypes = [C.c_int, C.c_int, P, P, P, P, P, P, P, P, P]
+        L.oracle_create_matrix.restype = P
+        L.oracle_assembled_free.argtypes = [P]
+        L.oracle_assembled_block.argtypes = [P, C.c_int, C.c_int, C.POINTER(P)]
+        L.oracle_assembled_block.restype = I64
         _lib = L
     return _lib
 
@@ -209,3 +214,56 @@ def petsc_read(filename, P: int):
         return out
     finally:
         L.oracle_petsc_free(h)
+
+
+def create_matrix(blocks, nrows_local, ncols_local, row_ghosts, col_ghosts):
+    """Matrix::create_matrix restated (Matrix.cpp:213-438): per rank
+    [rowptr, colind, values, ghosts] of the assembled matrix (values in the
+    blocks' dtype: float64 or complex128)."""
+    L = lib()
+    P = len(blocks)
+    cplx = np.iscomplexobj(blocks[0][2])
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dt)
+        keep.append(a)
+        return a.ctypes.data if len(a) else None
+
+    def parr(addrs):
+        out = (C.c_void_p * max(1, len(addrs)))()
+        for i, a in enumerate(addrs):
+            out[i] = a
+        return out
+
+    rp = parr([arr(b[0], np.int32) for b in blocks])
+    ci = parr([arr(b[1], np.int32) for b in blocks])
+    va = parr([arr(b[2], np.complex128 if cplx else np.float64) for b in blocks])
+    rg = parr([arr(g, np.int64) for g in row_ghosts])
+    cg_ = parr([arr(g, np.int64) for g in col_ghosts])
+    i64 = lambda v: (C.c_int64 * P)(*[int(t) for t in v])  # noqa: E731
+    h = L.oracle_create_matrix(P, 1 if cplx else 0, i64(nrows_local), i64(ncols_local), rp, ci,
+                               va, rg, i64([len(g) for g in row_ghosts]), cg_,
+                               i64([len(g) for g in col_ghosts]))
+    if not h:
+        raise RuntimeError(L.oracle_last_error().decode())
+    try:
+        out = []
+        for r in range(P):
+            arrs = []
+            for field, ct, dt in ((0, C.c_int32, np.int32), (1, C.c_int32, np.int32),
+                                  (2, C.c_double, np.float64), (3, C.c_int64, np.int64)):
+                p = C.c_void_p()
+                n = L.oracle_assembled_block(h, r, field, C.byref(p))
+                m = 2 * n if field == 2 else n
+                a = (np.ctypeslib.as_array(C.cast(p, C.POINTER(ct)), (m,)).copy()
+                     if n > 0 else np.zeros(m, dt))
+                if field == 2:
+                    a = a.view(np.complex128)
+                    if not cplx:
+                        a = a.real.copy()
+                arrs.append(a)
+            out.append(arrs)
+        return out
+    finally:
+        L.oracle_assembled_free(h)

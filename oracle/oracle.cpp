@@ -27,6 +27,7 @@
 #include <iterator>
 #include <map>
 #include <memory>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -652,6 +653,222 @@ int64_t oracle_petsc_block(oracle_petsc h, int rank, int field, const void** dat
     case 1: *data = B.colind.data(); return int64_t(B.colind.size());
     case 2: *data = B.vals.data(); return int64_t(B.vals.size());
     case 3: *data = B.ghosts.data(); return int64_t(B.ghosts.size());
+  }
+  *data = nullptr;
+  return -1;
+}
+
+// Matrix::create_matrix (Matrix.cpp:213-438) restated for all P ranks.
+// The MPI steps are restated by what they deliver: the Allgathers give the
+// prefix ranges; each rank's ghost rows are packed per destination (the
+// sorted std::set of owners) as {row, nnz, cols...} / {0, 0, vals...}; the
+// neighbourhood alltoallv hands receiver q the segments of its sources in
+// ascending rank order.  Eigen's setFromTriplets is restated by its steps: a
+// column-major copy filled in triplet order, duplicates collapsed per column
+// into the first occurrence (summed in order), then the transposed copy back
+// to row-major (rows in ascending column order).
+}  // extern "C"
+
+typedef struct OracleAssembled* oracle_assembled;
+struct OracleAssembled {
+  std::vector<std::vector<int32_t>> rowptr, colind;
+  std::vector<std::vector<std::complex<double>>> vals;
+  std::vector<std::vector<int64_t>> ghosts;
+};
+
+template <typename T>
+static void create_matrix_restated(int P, const int64_t* nrows_local, const int64_t* ncols_local,
+                                   const int32_t* const* Aouter_all,
+                                   const int32_t* const* Ainner_all, const T* const* Aval_all,
+                                   const int64_t* const* row_ghosts_all,
+                                   const int64_t* n_row_ghosts,
+                                   const int64_t* const* col_ghosts_all,
+                                   const int64_t* n_col_ghosts, OracleAssembled& out) {
+  std::vector<int64_t> row_ranges(P + 1, 0), col_ranges(P + 1, 0);
+  for (int i = 0; i < P; ++i) {
+    row_ranges[i + 1] = row_ranges[i] + nrows_local[i];
+    col_ranges[i + 1] = col_ranges[i] + ncols_local[i];
+  }
+  // Send side, per rank.
+  std::vector<std::vector<int>> dests(P);
+  std::vector<std::vector<int64_t>> send_index(P);
+  std::vector<std::vector<T>> send_val(P);
+  std::vector<std::vector<int>> send_offset(P);
+  for (int rank = 0; rank < P; ++rank) {
+    const int64_t ng = n_row_ghosts[rank];
+    std::vector<int> row_owner(ng);
+    for (int64_t i = 0; i < ng; ++i) {
+      auto it = std::upper_bound(row_ranges.begin(), row_ranges.end(), row_ghosts_all[rank][i]);
+      row_owner[i] = int(it - row_ranges.begin()) - 1;
+    }
+    std::set<int> neighbour_set(row_owner.begin(), row_owner.end());
+    dests[rank].assign(neighbour_set.begin(), neighbour_set.end());
+    std::map<int, int> proc_to_dest;
+    for (size_t i = 0; i < dests[rank].size(); ++i) proc_to_dest.insert({dests[rank][i], int(i)});
+    for (auto& q : row_owner) q = proc_to_dest[q];
+    const int32_t* Aouter = Aouter_all[rank];
+    const int32_t* Ainner = Ainner_all[rank];
+    const T* Aval = Aval_all[rank];
+    const int64_t nrl = nrows_local[rank], ncl = ncols_local[rank];
+    std::vector<std::vector<int64_t>> p_to_index(dests[rank].size());
+    std::vector<std::vector<T>> p_to_val(dests[rank].size());
+    for (int64_t i = 0; i < ng; ++i) {
+      const int p = row_owner[i];
+      p_to_index[p].push_back(row_ghosts_all[rank][i]);
+      p_to_val[p].push_back(T(0));
+      p_to_index[p].push_back(Aouter[nrl + i + 1] - Aouter[nrl + i]);
+      p_to_val[p].push_back(T(0));
+      for (int j = Aouter[nrl + i]; j < Aouter[nrl + i + 1]; ++j) {
+        const int64_t gi = Ainner[j] < ncl ? Ainner[j] + col_ranges[rank]
+                                           : col_ghosts_all[rank][Ainner[j] - ncl];
+        p_to_index[p].push_back(gi);
+        p_to_val[p].push_back(Aval[j]);
+      }
+    }
+    send_offset[rank] = {0};
+    for (size_t p = 0; p < dests[rank].size(); ++p) {
+      send_index[rank].insert(send_index[rank].end(), p_to_index[p].begin(), p_to_index[p].end());
+      send_val[rank].insert(send_val[rank].end(), p_to_val[p].begin(), p_to_val[p].end());
+      send_offset[rank].push_back(int(send_index[rank].size()));
+    }
+  }
+  out.rowptr.assign(P, {});
+  out.colind.assign(P, {});
+  out.vals.assign(P, {});
+  out.ghosts.assign(P, {});
+  for (int rank = 0; rank < P; ++rank) {
+    // Receive: sources in ascending rank order, each its segment for us.
+    std::vector<int64_t> recv_index;
+    std::vector<T> recv_val;
+    for (int src = 0; src < P; ++src) {
+      const auto& d = dests[src];
+      auto it = std::find(d.begin(), d.end(), rank);
+      if (it == d.end()) continue;
+      const int k = int(it - d.begin());
+      recv_index.insert(recv_index.end(), send_index[src].begin() + send_offset[src][k],
+                        send_index[src].begin() + send_offset[src][k + 1]);
+      recv_val.insert(recv_val.end(), send_val[src].begin() + send_offset[src][k],
+                      send_val[src].begin() + send_offset[src][k + 1]);
+    }
+    const int64_t nrl = nrows_local[rank], ncl = ncols_local[rank];
+    std::map<int64_t, int> col_ghost_map;
+    for (int64_t i = 0; i < n_col_ghosts[rank]; ++i)
+      col_ghost_map.insert({col_ghosts_all[rank][i], -1});
+    size_t pos = 0;
+    while (pos < recv_index.size()) {
+      ++pos;
+      const int nnz = int(recv_index[pos]);
+      ++pos;
+      for (int k = 0; k < nnz; ++k) {
+        const int64_t recv_col = recv_index[pos++];
+        if (recv_col >= col_ranges[rank + 1] || recv_col < col_ranges[rank])
+          col_ghost_map.insert({recv_col, -1});
+      }
+    }
+    int c = int(ncl);
+    for (auto& q : col_ghost_map) q.second = c++;
+    struct Trip {
+      int row, col;
+      T val;
+    };
+    std::vector<Trip> mat_data;
+    const int32_t* Aouter = Aouter_all[rank];
+    const int32_t* Ainner = Ainner_all[rank];
+    for (int row = 0; row < nrl; ++row)
+      for (int j = Aouter[row]; j < Aouter[row + 1]; ++j) {
+        int col = Ainner[j];
+        if (col >= ncl) col = col_ghost_map.find(col_ghosts_all[rank][col - ncl])->second;
+        mat_data.push_back({row, col, Aval_all[rank][j]});
+      }
+    pos = 0;
+    while (pos < recv_index.size()) {
+      const int row = int(recv_index[pos] - row_ranges[rank]);
+      ++pos;
+      const int nnz = int(recv_index[pos]);
+      ++pos;
+      for (int k = 0; k < nnz; ++k) {
+        const int64_t gc = recv_index[pos];
+        const T val = recv_val[pos];
+        ++pos;
+        const int col = (gc >= col_ranges[rank + 1] || gc < col_ranges[rank])
+                            ? col_ghost_map.find(gc)->second
+                            : int(gc - col_ranges[rank]);
+        mat_data.push_back({row, col, val});
+      }
+    }
+    // setFromTriplets: column-major lists in triplet order.
+    const int ncols = c;
+    std::vector<std::vector<std::pair<int, T>>> tr(ncols);
+    for (const Trip& t : mat_data) tr[t.col].push_back({t.row, t.val});
+    // collapseDuplicates per column: first occurrence keeps the running sum.
+    std::vector<int> wi(nrl, -1);
+    for (int j = 0; j < ncols; ++j) {
+      std::vector<std::pair<int, T>> kept;
+      for (const auto& e : tr[j]) {
+        if (wi[e.first] >= 0 && size_t(wi[e.first]) < kept.size() &&
+            kept[wi[e.first]].first == e.first) {
+          kept[wi[e.first]].second = kept[wi[e.first]].second + e.second;
+        } else {
+          wi[e.first] = int(kept.size());
+          kept.push_back(e);
+        }
+      }
+      for (const auto& e : kept) wi[e.first] = -1;
+      tr[j] = std::move(kept);
+    }
+    // Transposed copy to row-major: rows in ascending column order.
+    std::vector<std::vector<std::pair<int, T>>> rows(nrl);
+    for (int j = 0; j < ncols; ++j)
+      for (const auto& e : tr[j]) rows[e.first].push_back({j, e.second});
+    auto& rp = out.rowptr[rank];
+    rp.push_back(0);
+    for (const auto& rv : rows) {
+      for (const auto& e : rv) {
+        out.colind[rank].push_back(e.first);
+        out.vals[rank].push_back(std::complex<double>(e.second));
+      }
+      rp.push_back(int32_t(out.colind[rank].size()));
+    }
+    for (auto& q : col_ghost_map) out.ghosts[rank].push_back(q.first);
+  }
+}
+
+extern "C" {
+
+// dtype: 0 float64, 1 complex128 (values interleaved).
+oracle_assembled oracle_create_matrix(int P, int dtype, const int64_t* nrows_local,
+                                      const int64_t* ncols_local, const int32_t* const* rowptr,
+                                      const int32_t* const* colind, const void* const* values,
+                                      const int64_t* const* row_ghosts,
+                                      const int64_t* n_row_ghosts,
+                                      const int64_t* const* col_ghosts,
+                                      const int64_t* n_col_ghosts) {
+  oracle_assembled h = nullptr;
+  const int st = guard([&] {
+    std::unique_ptr<OracleAssembled> out(new OracleAssembled);
+    if (dtype == 0)
+      create_matrix_restated<double>(P, nrows_local, ncols_local, rowptr, colind,
+                                     reinterpret_cast<const double* const*>(values), row_ghosts,
+                                     n_row_ghosts, col_ghosts, n_col_ghosts, *out);
+    else
+      create_matrix_restated<std::complex<double>>(
+          P, nrows_local, ncols_local, rowptr, colind,
+          reinterpret_cast<const std::complex<double>* const*>(values), row_ghosts,
+          n_row_ghosts, col_ghosts, n_col_ghosts, *out);
+    h = out.release();
+  });
+  return st == 0 ? h : nullptr;
+}
+
+void oracle_assembled_free(oracle_assembled h) { delete h; }
+
+// field: 0 rowptr, 1 colind (int32), 2 values (complex128 pairs), 3 ghosts.
+int64_t oracle_assembled_block(oracle_assembled h, int rank, int field, const void** data) {
+  switch (field) {
+    case 0: *data = h->rowptr[rank].data(); return int64_t(h->rowptr[rank].size());
+    case 1: *data = h->colind[rank].data(); return int64_t(h->colind[rank].size());
+    case 2: *data = h->vals[rank].data(); return int64_t(h->vals[rank].size());
+    case 3: *data = h->ghosts[rank].data(); return int64_t(h->ghosts[rank].size());
   }
   *data = nullptr;
   return -1;

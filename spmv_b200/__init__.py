@@ -6,8 +6,8 @@ the package does not build or load anything, and every compute call fails
 loudly if ``libspmv_b200.so`` is missing (there is no CPU fallback).
 """
 from ._lib import SpmvError  # noqa: F401
-from .core import (Comm, L2GMap, Matrix, cg, cg_mixed, owner_ranges,  # noqa: F401
-                   read_petsc_binary, read_petsc_binary_vector)
+from .core import (Comm, L2GMap, Matrix, cg, cg_mixed, create_matrix,  # noqa: F401
+                   owner_ranges, read_petsc_binary, read_petsc_binary_vector)
 
-__all__ = ["Comm", "L2GMap", "Matrix", "cg", "cg_mixed", "SpmvError", "owner_ranges",
-           "read_petsc_binary", "read_petsc_binary_vector"]
+__all__ = ["Comm", "L2GMap", "Matrix", "cg", "cg_mixed", "create_matrix", "SpmvError",
+           "owner_ranges", "read_petsc_binary", "read_petsc_binary_vector"]

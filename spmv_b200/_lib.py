@@ -120,6 +120,9 @@ _SIGS = {
     "spmv_matrix_mult_block": [_p, _int, _int, _pp, _pp],
     "spmv_cg_block": [_p, _int, _int, _pp, _pp, _int, C.c_double, C.POINTER(CgInfo)],
     "spmv_owner_ranges": [_int, _i64, C.POINTER(_i64)],
+    "spmv_matrix_create_assembled": [_p, _int, C.POINTER(_i64), C.POINTER(_i64), _pp, _pp, _pp,
+                                     _pp, C.POINTER(_i64), _pp, C.POINTER(_i64), C.POINTER(_p),
+                                     C.POINTER(_p), C.POINTER(_p)],
     "spmv_petsc_read_matrix": [_p, C.c_char_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p)],
     "spmv_petsc_vector_size": [C.c_char_p, C.POINTER(_i64)],
     "spmv_petsc_read_vector": [_p, C.c_char_p, _pp],

@@ -535,16 +535,51 @@ def read_petsc_binary(comm: Comm, filename: str) -> Matrix:
     cm, rm, h = C.c_void_p(), C.c_void_p(), C.c_void_p()
     call("spmv_petsc_read_matrix", comm.handle, str(filename).encode(), C.byref(cm),
          C.byref(rm), C.byref(h))
+    return _adopt_matrix(comm, cm, rm, h, np.dtype(np.float64))
+
+
+def _adopt_matrix(comm: Comm, cm, rm, h, np_dtype) -> Matrix:
+    """A Matrix (and its two maps) around handles the caller now owns."""
     col_map = L2GMap.__new__(L2GMap)
     col_map.comm, col_map._h = comm, cm
     row_map = L2GMap.__new__(L2GMap)
     row_map.comm, row_map._h = comm, rm
     M = Matrix.__new__(Matrix)
     M.comm, M._col_map, M._row_map, M._h = comm, col_map, row_map, h
-    M.np_dtype, M.dtype = np.dtype(np.float64), _lib.FLOAT64
+    M.np_dtype, M.dtype = np_dtype, _DTYPES[np_dtype]
     M.nrows = [row_map.local_size(r) for r in range(comm.size)]
     M.ncols = [col_map.vec_len(r) for r in range(comm.size)]
     return M
+
+
+def create_matrix(comm: Comm, blocks, nrows_local: Sequence[int], ncols_local: Sequence[int],
+                  row_ghosts: Sequence[Sequence[int]],
+                  col_ghosts: Sequence[Sequence[int]]) -> Matrix:
+    """Matrix::create_matrix (Matrix.cpp:213-438) for every rank: blocks[r]
+    = (rowptr, colind, values) with nrows_local[r] owned rows then one row
+    per row_ghosts[r] entry, columns owned first then col_ghosts[r].  Ghost
+    rows are summed into their owners; returns the assembled matrix, whose
+    .col_map() / .row_map() are its maps."""
+    P = comm.size
+    rps = [np.ascontiguousarray(b[0], np.int32) for b in blocks]
+    cis = [np.ascontiguousarray(b[1], np.int32) for b in blocks]
+    vas = [np.ascontiguousarray(b[2]) for b in blocks]
+    dts = {v.dtype for v in vas}
+    if len(blocks) != P or len(dts) != 1 or next(iter(dts)) not in _DTYPES:
+        raise SpmvError(_lib.ERROR_INVALID_ARGUMENT,
+                        "spmv::Matrix::create_matrix - Error: one block per rank, one dtype")
+    npdt = next(iter(dts))
+    rg = [np.ascontiguousarray(np.asarray(g, dtype=np.int64)) for g in row_ghosts]
+    cg_ = [np.ascontiguousarray(np.asarray(g, dtype=np.int64)) for g in col_ghosts]
+    i64 = lambda v: (C.c_int64 * P)(*[int(t) for t in v])  # noqa: E731
+    cm, rm, h = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    call("spmv_matrix_create_assembled", comm.handle, _DTYPES[npdt], i64(nrows_local),
+         i64(ncols_local), ptr_array([a.ctypes.data for a in rps]),
+         ptr_array([a.ctypes.data for a in cis]), ptr_array([a.ctypes.data for a in vas]),
+         ptr_array([g.ctypes.data if len(g) else None for g in rg]), i64([len(g) for g in rg]),
+         ptr_array([g.ctypes.data if len(g) else None for g in cg_]),
+         i64([len(g) for g in cg_]), C.byref(cm), C.byref(rm), C.byref(h))
+    return _adopt_matrix(comm, cm, rm, h, npdt)
 
 
 def read_petsc_binary_vector(comm: Comm, filename: str) -> List[np.ndarray]:

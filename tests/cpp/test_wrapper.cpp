@@ -43,6 +43,29 @@ int main(int argc, char** argv) {
     EXPECT(m.global_offset(1) == 4 && m.global_to_local(0, 4) == 4);
     EXPECT(m.ghosts(1).size() == 1 && m.ghosts(1)[0] == 3);
   }
+  {
+    // create_matrix: two ranks of a 4-point chain, rank 0 owns rows 0-1 and
+    // holds a ghost row for node 2 (owned by rank 1) with entries in columns
+    // 1 (owned) and 2 (a ghost column); rank 1 adds its own row 2 entry.
+    spmv::Comm comm(2, -1);
+    std::vector<spmv::CsrBlock<double>> blocks(2);
+    blocks[0].rowptr = {0, 1, 2, 4};       // rows 0, 1 and ghost row 2
+    blocks[0].colind = {0, 1, 1, 2};       // local col 2 = global 2
+    blocks[0].values = {1.0, 2.0, 3.0, 4.0};
+    blocks[1].rowptr = {0, 1, 2};          // rows 2, 3
+    blocks[1].colind = {0, 1};
+    blocks[1].values = {10.0, 20.0};
+    auto A = spmv::Matrix<double>::create_matrix(comm, blocks, {2, 2}, {2, 2}, {{2}, {}},
+                                                 {{2}, {}});
+    // Rank 1, row 0 (global 2): own entry 10 at col 0, plus received 4.0 at
+    // global 2 (= local 0, summed: 14) and 3.0 at global 1 (a new ghost).
+    const std::int32_t *rp = nullptr, *ci = nullptr;
+    const void* va = nullptr;
+    spmv::detail::check(spmv_matrix_csr(A.handle(), 1, &rp, &ci, &va));
+    const double* v = static_cast<const double*>(va);
+    EXPECT(rp[1] == 2 && ci[0] == 0 && v[0] == 14.0 && ci[1] == 2 && v[1] == 3.0);
+    EXPECT(A.col_map()->num_ghosts(1) == 1 && A.col_map()->ghosts(1)[0] == 1);
+  }
   if (argc > 2) {
     // argv[2]: a PETSc binary file of the 5x5 matrix with A[i][j] = 10 i + j
     // on |i - j| <= 1, rows written with descending columns; argv[3] the
