@@ -308,6 +308,100 @@ def run_extras(device: int, reps: int, c4_count: int):
     out["c5_adjoint"] = {"forward_plus_adjoint_s": ta,
                          "cg_iterations": sysm.last_iterations[-2:],
                          "edges": int(2 * 1024 * 1023)}
+    del sysm, bt, xs, vals
+    torch.cuda.empty_cache()
+    out.update(run_next_rows(device, reps))
+    return out
+
+
+def run_next_rows(device: int, reps: int):
+    """The rows beyond the CG path, on the c2 matrix (3D 7-point 128^3, 8
+    ranks): complex128 Matrix::mult (GB/s against the measured HBM peak),
+    the PETSc binary reader (file written untimed, read timed, host), and
+    create_matrix on a 5-point assembly of a 512^2 node grid over 8 ranks,
+    each rank also holding the next grid line's rows (host)."""
+    import tempfile
+    import torch
+    import spmv_b200 as S
+    from spmv_b200 import gen, petsc
+    out = {}
+    hbm, src = peaks()
+    W = gen.workload(WORKLOAD)
+    D = gen.distribute(W.A, W.P)
+    P = W.P
+    n, nnz = W.A.nrows, W.A.nnz
+    g = int(sum(len(x) for x in D.ghosts))
+    # complex128 mult -----------------------------------------------------
+    comm = S.Comm(size=P, device=device)
+    stream = comm.torch_stream()
+    cm = S.L2GMap(comm, D.local_sizes, D.ghosts)
+    rm = S.L2GMap(comm, D.local_sizes, [[] for _ in range(P)])
+    rng = np.random.default_rng(12)
+    blocks = [(rp, ci, (va + 1j * rng.standard_normal(len(va))).astype(np.complex128))
+              for rp, ci, va in D.blocks]
+    Mc = S.Matrix(comm, blocks, cm, rm)
+    Mc.autotune(reps=5)
+    xs = [torch.complex(torch.rand(cm.vec_len(q), dtype=torch.float64, device=f"cuda:{device}"),
+                        torch.rand(cm.vec_len(q), dtype=torch.float64, device=f"cuda:{device}"))
+          for q in range(P)]
+    ys = [torch.empty(D.local_sizes[q], dtype=torch.complex128, device=f"cuda:{device}")
+          for q in range(P)]
+    t, _ = _timed(stream, lambda: Mc.mult(xs, out=ys), max(reps, 20))
+    kb = kernel_bytes(n, nnz, P, g, sv=16)
+    out["complex128_mult_c2"] = {"us_per_launch": t * 1e6, "bytes_per_launch": kb,
+                                 "gbs": kb / t / 1e9, "frac_of_measured_hbm": kb / t / 1e9 / hbm,
+                                 "kernel": Mc.get_kernel()}
+    del Mc, xs, ys, blocks
+    torch.cuda.empty_cache()
+    # PETSc reader ----------------------------------------------------------
+    with tempfile.TemporaryDirectory() as d:
+        fa = f"{d}/A.dat"
+        petsc.write_matrix(fa, W.A.rowptr, W.A.cols, W.A.vals, W.A.ncols)
+        size = os.path.getsize(fa)
+        t0 = time.perf_counter()
+        A = S.read_petsc_binary(S.Comm(size=P, device=device), fa)
+        tr = time.perf_counter() - t0
+        same = all(np.array_equal(A.mat(q)[1], D.blocks[q][1]) for q in range(P))
+        out["petsc_read_c2"] = {"seconds": tr, "file_bytes": size,
+                                "file_mb_per_s": size / tr / 1e6,
+                                "blocks_equal_workload_distribution": bool(same)}
+        del A
+    # create_matrix -----------------------------------------------------------
+    nx = 512
+    nodes = nx * nx
+    rr = S.owner_ranges(P, nodes)
+    bl, nrl, rgs, cgs = [], [], [], []
+    for r in range(P):
+        r0, r1 = rr[r], rr[r + 1]
+        # Rank r assembles the quads whose lowest node it owns: rows of its own
+        # nodes and of the next grid line (ghost rows owned by rank r + 1).
+        j0, j1 = r0 // nx, min((r1 + nx - 1) // nx, nx - 1)
+        rows = np.arange(j0 * nx, min((j1 + 1) * nx, nodes))
+        ghost_rows = rows[(rows < r0) | (rows >= r1)]
+        rowlist = np.concatenate([np.arange(r0, r1), ghost_rows])
+        # 5-point couplings of each listed row, each entry from two elements
+        # (repeats summed by the assembly).
+        cols, rptr = [], [0]
+        for gr in rowlist:
+            i, j = gr % nx, gr // nx
+            nb = [gr] + [q for q, ok in ((gr - 1, i > 0), (gr + 1, i < nx - 1),
+                                         (gr - nx, j > 0), (gr + nx, j < nx - 1)) if ok]
+            cols.extend(nb + nb)
+            rptr.append(len(cols))
+        cols = np.array(cols, np.int64)
+        gh = np.unique(cols[(cols < r0) | (cols >= r1)])
+        loc = np.where((cols >= r0) & (cols < r1), cols - r0, (r1 - r0) + np.searchsorted(gh, cols))
+        bl.append((np.array(rptr, np.int32), loc.astype(np.int32),
+                   np.full(len(cols), 0.5)))
+        nrl.append(r1 - r0)
+        rgs.append(ghost_rows.astype(np.int64))
+        cgs.append(gh)
+    t0 = time.perf_counter()
+    Ma = S.create_matrix(S.Comm(size=P, device=device), bl, nrl, nrl, rgs, cgs)
+    ta = time.perf_counter() - t0
+    out["create_matrix_512sq"] = {"seconds": ta, "rows": nodes,
+                                   "entries_in": int(sum(len(b[1]) for b in bl)),
+                                   "entries_out": int(sum(Ma.nnz(q) for q in range(P)))}
     return out
 
 
