@@ -22,6 +22,7 @@
 #include <cstring>
 #include <fstream>
 #include <numeric>
+#include <thread>
 
 #include "internal.h"
 
@@ -96,7 +97,9 @@ void read_petsc_matrix(const char* filename, int P, std::vector<PetscBlock>& blo
 
   const std::vector<int64_t> rr = owner_ranges(P, nrows), cr = owner_ranges(P, ncols);
   blocks.assign(size_t(P), PetscBlock{});
-  for (int r = 0; r < P; ++r) {
+  // One rank's block.  Rows already in ascending local order (the usual
+  // case) are copied straight; others are stably sorted.
+  auto build_block = [&](int r) {
     PetscBlock& B = blocks[r];
     const int64_t c0 = cr[r], c1 = cr[r + 1];
     const int64_t e0 = rowstart[rr[r]], e1 = rowstart[rr[r + 1]];
@@ -118,31 +121,56 @@ void read_petsc_matrix(const char* filename, int P, std::vector<PetscBlock>& blo
     B.rowptr.assign(size_t(B.nrows) + 1, 0);
     B.colind.resize(size_t(e1 - e0));
     B.vals.resize(size_t(e1 - e0));
-    std::vector<int32_t> order;
+    std::vector<int32_t> loc, order;
     for (int32_t i = 0; i < B.nrows; ++i) {
       const int64_t s = rowstart[rr[r] + i], e = rowstart[rr[r] + i + 1];
       B.rowptr[i + 1] = int32_t(e - e0);
-      // Local column of each entry, then a stable sort of the row by it.
-      std::vector<int32_t> loc(size_t(e - s));
+      loc.resize(size_t(e - s));
+      bool sorted = true;
       for (int64_t j = s; j < e; ++j) {
         const int64_t c = g[size_t(j - e0)];
-        loc[size_t(j - s)] =
+        const int32_t l =
             c >= c0 && c < c1
                 ? int32_t(c - c0)
                 : int32_t(B.ncols_local +
                           (std::lower_bound(B.ghosts.begin(), B.ghosts.end(), c) - B.ghosts.begin()));
+        if (j > s && l < loc[size_t(j - s) - 1]) sorted = false;
+        loc[size_t(j - s)] = l;
+      }
+      int32_t* ci = B.colind.data() + (s - e0);
+      double* va = B.vals.data() + (s - e0);
+      if (sorted) {
+        for (int64_t j = s; j < e; ++j) {
+          ci[j - s] = loc[size_t(j - s)];
+          va[j - s] = be64(vbuf.data() + 8 * j);
+        }
+        continue;
       }
       order.resize(loc.size());
       std::iota(order.begin(), order.end(), 0);
       std::stable_sort(order.begin(), order.end(),
                        [&](int32_t a, int32_t b) { return loc[a] < loc[b]; });
       for (size_t k = 0; k < order.size(); ++k) {
-        const int64_t j = s + order[k];
-        B.colind[size_t(s - e0) + k] = loc[order[k]];
-        B.vals[size_t(s - e0) + k] = be64(vbuf.data() + 8 * j);
+        ci[k] = loc[order[k]];
+        va[k] = be64(vbuf.data() + 8 * (s + order[k]));
       }
     }
-  }
+  };
+  // Ranks are independent: one host thread each; the first error (in rank
+  // order) is reported.
+  std::vector<std::string> errs(static_cast<size_t>(P));
+  std::vector<std::thread> pool;
+  for (int r = 0; r < P; ++r)
+    pool.emplace_back([&, r] {
+      try {
+        build_block(r);
+      } catch (const std::exception& e) {
+        errs[r] = e.what();
+      }
+    });
+  for (auto& t : pool) t.join();
+  for (const std::string& e : errs)
+    if (!e.empty()) fail(SPMV_ERROR_INVALID_ARGUMENT, e);
   if (nrows_out) *nrows_out = nrows;
   if (ncols_out) *ncols_out = ncols;
 }
