@@ -243,7 +243,12 @@ K1Fn k1_sell(int U) {
 
 template <bool D16, bool H>
 K1Fn k1_staged(int U) {
-  return U >= 8 ? cg_k1_staged<8, D16, H> : cg_k1_staged<4, D16, H>;
+  switch (staged_width(U)) {
+    case 8: return cg_k1_staged<8, D16, H>;
+    case 7: return cg_k1_staged<7, D16, H>;
+    case 5: return cg_k1_staged<5, D16, H>;
+    default: return cg_k1_staged<4, D16, H>;
+  }
 }
 
 template <bool H>

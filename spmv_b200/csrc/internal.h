@@ -339,6 +339,9 @@ enum class ProductKind : int {
   Sell = 1,    // SELL-32 from registers, w loads in flight per lane
   Staged = 2,  // SELL-32 staged in shared memory by bulk copies, w gathers per lane
 };
+// Gathers in flight per lane of the staged product: 4, 8, or a stencil's
+// exact row width 5 or 7 (one unmasked chunk per slice).
+inline int staged_width(int w) { return w >= 8 ? 8 : (w == 7 || w == 5) ? w : 4; }
 struct SolverProduct {
   ProductKind kind = ProductKind::Vector;
   int w = 0;

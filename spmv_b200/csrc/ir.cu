@@ -300,7 +300,14 @@ using KR = void (*)(SpmvArgs, IrPtrs);
 // lane (1..16), staged gathers in flight per lane (4 or 8).
 template <int KIND, bool D16, bool H>
 K1 pick_k1(int W) {
-  if (KIND == 2) return W >= 8 ? ir_spmv_dot<8, KIND, D16, H> : ir_spmv_dot<4, KIND, D16, H>;
+  if (KIND == 2) {
+    switch (staged_width(W)) {
+      case 8: return ir_spmv_dot<8, KIND, D16, H>;
+      case 7: return ir_spmv_dot<7, KIND, D16, H>;
+      case 5: return ir_spmv_dot<5, KIND, D16, H>;
+      default: return ir_spmv_dot<4, KIND, D16, H>;
+    }
+  }
   switch (W) {
     case 1: return ir_spmv_dot<1, KIND, D16, H>;
     case 2: return ir_spmv_dot<2, KIND, D16, H>;
@@ -313,7 +320,14 @@ K1 pick_k1(int W) {
 }
 template <int KIND, bool D16>
 KR pick_kr(int W) {
-  if (KIND == 2) return W >= 8 ? ir_residual<8, KIND, D16> : ir_residual<4, KIND, D16>;
+  if (KIND == 2) {
+    switch (staged_width(W)) {
+      case 8: return ir_residual<8, KIND, D16>;
+      case 7: return ir_residual<7, KIND, D16>;
+      case 5: return ir_residual<5, KIND, D16>;
+      default: return ir_residual<4, KIND, D16>;
+    }
+  }
   switch (W) {
     case 1: return ir_residual<1, KIND, D16>;
     case 2: return ir_residual<2, KIND, D16>;

@@ -369,8 +369,11 @@ __global__ void __launch_bounds__(SolverStaged::BS)
 template <typename T>
 void launch_staged_t(const SpmvLaunch& L, const SpmvArgs& a, const DevCsr::StagedTable& t,
                      int U, cudaStream_t s) {
-  const void* fn = U >= 8 ? (const void*)spmv_staged_kernel<T, int32_t, 8>
-                          : (const void*)spmv_staged_kernel<T, int32_t, 4>;
+  const int u = staged_width(U);
+  const void* fn = u == 8   ? (const void*)spmv_staged_kernel<T, int32_t, 8>
+                   : u == 7 ? (const void*)spmv_staged_kernel<T, int32_t, 7>
+                   : u == 5 ? (const void*)spmv_staged_kernel<T, int32_t, 5>
+                            : (const void*)spmv_staged_kernel<T, int32_t, 4>;
   const StagedShape sh = staged_shape(fn, int(sizeof(T)) + 4, t.ntiles, L.num_sms);
   const StagedDesc* tiles = t.desc.as<StagedDesc>();
   int ntiles = t.ntiles;
@@ -388,7 +391,9 @@ void launch_staged(const SpmvLaunch& L, cudaStream_t stream) {
   const int eb = int(es) + 4;
   const DevCsr::StagedTable& t = staged_table(C, eb, SolverStaged::max_entries(eb));
   if (!t.ok) {
-    launch_sell(L, C.sell_cols.as<int32_t>(), stream);
+    SpmvLaunch Ls = L;
+    Ls.width = 0;  // the staged width means gathers in flight, not SELL loads
+    launch_sell(Ls, C.sell_cols.as<int32_t>(), stream);
     return;
   }
   SpmvArgs a;

@@ -163,10 +163,14 @@ SolverProduct choose_solver_product(spmv_matrix A, spmv_dtype dt, const void* x,
     if (want_staged) {
       const int eb = int(es) + (d ? 2 : 4);
       if (staged_table(A->fwd, eb, SolverStaged::max_entries(eb)).ok) {
-        if (only && A->width > 0)
-          cands.push_back({ProductKind::Staged, A->width >= 8 ? 8 : 4, d, 0.f});
-        else
+        if (only && A->width > 0) {
+          cands.push_back({ProductKind::Staged, staged_width(A->width), d, 0.f});
+        } else {
           for (int u : {4, 8}) cands.push_back({ProductKind::Staged, u, d, 0.f});
+          // A stencil whose rows all have 5 or 7 entries: one unmasked chunk.
+          if (C.max_row == 5 || C.max_row == 7)
+            cands.push_back({ProductKind::Staged, int(C.max_row), d, 0.f});
+        }
       }
     }
   }
@@ -247,12 +251,10 @@ int max_blocks_for(int num_sms, int BS) {
   return std::max(1, num_sms) * (2048 / BS) * 2;
 }
 
-void launch_spmv(const SpmvLaunch& L, cudaStream_t stream) {
+void launch_spmv(const SpmvLaunch& L0, cudaStream_t stream) {
+  SpmvLaunch L = L0;
   const bool cplx = L.dtype == SPMV_COMPLEX64 || L.dtype == SPMV_COMPLEX128;
-  const int W = L.width > 0 ? L.width : auto_width(L.csr->mean_row, L.dtype);
   const int BS = L.block > 0 ? L.block : 256;
-  require(W >= 1 && W <= 32 && (W & (W - 1)) == 0,
-          "spmv: width must be 1..32, a power of two");
   require(BS == 128 || BS == 256 || BS == 512,
           "spmv: block must be 128, 256 or 512");
   spmv_kernel k = pick_kernel(L.kernel, *L.csr, L.csr->sell_built);
@@ -260,6 +262,10 @@ void launch_spmv(const SpmvLaunch& L, cudaStream_t stream) {
   // pipeline are real only).
   if (cplx && k == SPMV_KERNEL_MERGE) k = SPMV_KERNEL_VECTOR;
   if (cplx && k == SPMV_KERNEL_STAGED) k = SPMV_KERNEL_SELL;
+  // A width belongs to the kernel it was chosen for (lanes per row, loads or
+  // gathers in flight); a fallback to another kernel uses its own default.
+  const bool same_kind = k == L.kernel || L.kernel == SPMV_KERNEL_AUTO;
+  if (!same_kind) L.width = 0;
   if (k == SPMV_KERNEL_MERGE) {
     require(L.carry != nullptr, "spmv: merge-path product needs a carry buffer");
     launch_merge(L, stream, *L.carry);
@@ -273,6 +279,9 @@ void launch_spmv(const SpmvLaunch& L, cudaStream_t stream) {
     launch_staged(L, stream);
     return;
   }
+  const int W = L.width > 0 ? L.width : auto_width(L.csr->mean_row, L.dtype);
+  require(W >= 1 && W <= 32 && (W & (W - 1)) == 0,
+          "spmv: width must be 1..32, a power of two");
   SpmvArgs a;
   const size_t es = dtype_size(L.dtype);
   fill_spmv_args(a, *L.csr, L.cols, es, L.x, L.y, nullptr, BS / W,
