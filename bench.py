@@ -546,6 +546,7 @@ def run_ours(args, info):
     # offsets, which moves 2 bytes less per nonzero than counted.
     b_iter = kernel_bytes(n, nnz, 1, 0) + 9 * n * 8
     cg_kind, cg_w, cg_bits, cg_us = M.solver_product("cg")
+    cg_form = M.cg_form()
     ms_per_iter = t_local / args.steps / k_mean * 1e3
 
     cpu = None
@@ -585,10 +586,14 @@ def run_ours(args, info):
                    "gbs": b_iter / (ms_per_iter / 1e3) / 1e9,
                    "bytes_per_iter": b_iter,
                    "product": {"kernel": cg_kind, "width": cg_w, "index_bits": cg_bits,
-                               "plain_us": cg_us}},
+                               "plain_us": cg_us},
+                   "form": {"kind": cg_form[0], "ctas_per_sm": cg_form[1],
+                            "residual_in": cg_form[2]}},
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": int(args.steps * (1 + 3 * k_mean)),
+            # A graph solve launches an init kernel and three per iteration;
+            # a fused solve is one cooperative launch.
+            "gpu_launches": int(args.steps * (1 if cg_form[0] == "fused" else 1 + 3 * k_mean)),
             "clocks": clk,
         }
         if cpu:

@@ -312,6 +312,13 @@ int spmv_cg_ex(spmv_matrix A, spmv_memory memory, const double* const* b,
 int spmv_matrix_solver_product(spmv_matrix A, int solver, spmv_kernel* kernel,
                                int* width, int* index_bits, double* us);
 
+/* How spmv_cg runs on this matrix (chosen by timing when its workspace was
+ * built): *fused = 0 for a CUDA graph of three kernels per iteration, 1 for
+ * one cooperative launch per solve with *ctas_per_sm persistent CTAs per SM
+ * and the residual held in shared memory (*r_shared = 1) or global memory.
+ * Fails when spmv_cg has not run on the matrix.  No reference counterpart. */
+int spmv_matrix_cg_form(spmv_matrix A, int* fused, int* ctas_per_sm, int* r_shared);
+
 typedef struct spmv_ir_info {
   int iterations;   /* inner FP32 CG iterations                             */
   int refinements;  /* FP64 true-residual recomputations                    */

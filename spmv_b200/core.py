@@ -344,6 +344,17 @@ class Matrix:
              C.byref(bits), C.byref(us))
         return _lib.KERNEL_NAMES[k.value], w.value, bits.value, us.value
 
+    def cg_form(self):
+        """How cg runs on this matrix: ("graph", 0, None) for three kernels
+        per iteration in a CUDA graph, or ("fused", CTAs per SM, "smem" or
+        "global": where the residual lives) for one cooperative launch per
+        solve; fails if cg has not run on the matrix."""
+        f, cps, rs = C.c_int(), C.c_int(), C.c_int()
+        call("spmv_matrix_cg_form", self._h, C.byref(f), C.byref(cps), C.byref(rs))
+        if not f.value:
+            return "graph", 0, None
+        return "fused", cps.value, "smem" if rs.value else "global"
+
     def get_kernel(self):
         k, w, b = C.c_int(), C.c_int(), C.c_int()
         call("spmv_matrix_get_kernel", self._h, C.byref(k), C.byref(w), C.byref(b))

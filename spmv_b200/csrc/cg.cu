@@ -32,8 +32,16 @@
 // each with 32-bit columns or 16-bit offsets.  (Forming p inside K1, where
 // the product gathers it, saves K3's pass over p and r but doubles the
 // gathers; measured on the 7-point stencil it was slower.)
+//
+// With a staged product the whole solve can instead run as one cooperative
+// launch (cg_fused below: the same three phases per iteration separated by
+// grid barriers, the residual held in shared memory); the workspace times
+// both forms on the matrix and keeps the faster.
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
+#include <cstdlib>
+#include <string>
 #include <type_traits>
 
 #include "internal.h"
@@ -50,6 +58,13 @@ struct CgWorkspace {
   int64_t n = 0;
   spmvb::SolverProduct product;
   spmvb::DevBuf b, x, r, p, y, partials, state;
+  // Fused solve (one cooperative launch; see cg_fused).
+  bool fused = false;
+  const void* fused_fn = nullptr;
+  int fused_grid = 0, fused_block = 0, fused_smem = 0, fused_cps = 0;
+  bool fused_rs = false;
+  spmvb::DevBuf bar, partials2, ctas;
+  spmvb::SpmvArgs fused_args;
   const spmvb::StagedDesc* tiles = nullptr;
   int ntiles = 0;
   cudaGraph_t graph = nullptr;
@@ -79,6 +94,8 @@ struct CgPtrs {
   int64_t n;
   const StagedDesc* tiles;  // staged product only
   int ntiles;
+  unsigned long long* bar;  // fused solve: grid barrier counter
+  double* partials2;        // fused solve: second reduction's partials
 };
 
 __global__ void __launch_bounds__(EW_BS)
@@ -153,7 +170,7 @@ __global__ void __launch_bounds__(256)
 }
 
 template <int U, bool D16, bool H>
-__global__ void __launch_bounds__(SolverStaged::BS)
+__global__ void __launch_bounds__(SolverStaged::BS, SolverStaged::MINB)
     cg_k1_staged(const __grid_constant__ SpmvArgs a, const CgPtrs c,
                  cudaGraphConditionalHandle h) {
   if (H && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
@@ -212,6 +229,235 @@ __global__ void __launch_bounds__(EW_BS) cg_update_xp(const CgPtrs c) {
     st_pol(c.x + i, ld_pol(c.x + i, keep) + alpha * pi, keep);
     st_pol(c.p + i, pi * beta + ld_pol(c.r + i, keep), keep);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Fused solve: the whole of cg (init and every iteration) as one cooperative
+// launch of persistent CTAs, each owning a contiguous run of the staged
+// tiles and so a contiguous range [g0, g1) of the global rows.  Per
+// iteration, with grid barriers between the phases:
+//
+//   A  y = A p over the CTA's tiles (the staged traversal; its producer warp
+//      keeps streaming the same tiles pass after pass, so the next pass's
+//      first tiles land during B and C), p.y          -> barrier, alpha
+//   B  r -= alpha y, x += alpha p on the CTA's rows, r.r -> barrier, beta,
+//      count, convergence test (identical in every CTA)
+//   C  p = p beta + r on the CTA's rows               -> barrier (A gathers p)
+//
+// RS: r lives in shared memory for the whole solve (only this CTA's rows
+// ever read it), so it never crosses HBM.  The arithmetic of every vector
+// element is the graph form's; the two dot products are summed in a
+// different grouping (per-CTA partials over the CTA's rows).
+struct FusedCta {
+  int32_t t0, t1;  // tiles [t0, t1)
+  int32_t g0, g1;  // global rows [g0, g1)
+};
+
+// Phase A of the fused solve for one consumer thread: one pass of the staged
+// traversal, y = A p, returning this thread's share of p.y.
+template <class CFG, int U, typename CI>
+__device__ __forceinline__ double cg_fused_product(const SpmvArgs& a, int count, uint64_t q_base,
+                                                StagedLoop<CFG>& pipe,
+                                                const unsigned char* smem, int* err,
+                                                double* __restrict__ y,
+                                                const double* __restrict__ p) {
+  const uint64_t keep = l2_policy_keep();
+  double acc = 0.0;
+  staged_loop_consume<CFG, double, CI, U>(
+      a, count, q_base, pipe, smem, err,
+      [&](const PartArg& P, int row, double sum) {
+        const int g = P.row0 + row;
+        st_pol(y + g, sum, keep);
+        acc += ld_pol(p + g, keep) * sum;
+      },
+      XGather<double, true>());
+  return acc;
+}
+
+template <class CFG, int U, bool D16, bool RS>
+__global__ void __launch_bounds__(CFG::BS, CFG::MINB)
+    cg_fused(const __grid_constant__ SpmvArgs a, const CgPtrs c,
+             const FusedCta* __restrict__ ctas) {
+  using CI = typename std::conditional<D16, int16_t, int32_t>::type;
+  constexpr int NT = CFG::NC * 32;
+  constexpr int STAGES_BYTES = CFG::smem_bytes(8 + int(sizeof(CI)));
+  extern __shared__ __align__(128) unsigned char staged_smem[];
+  __shared__ StagedLoop<CFG> pipe;
+  __shared__ GridSum<NT> gs;
+  // Solver scalars, written by thread 0 between barriers (kept out of the
+  // registers the product phase needs).
+  __shared__ struct {
+    double rnorm0, rnorm_old, rnorm_new, alpha, beta, pdoty, rtol2;
+    int kmax, k, status, go;
+  } sv;
+
+  const FusedCta me = ctas[blockIdx.x];
+  const int count = me.t1 - me.t0;
+  const int tid = int(threadIdx.x);
+  if (tid == 0) staged_loop_init(pipe);
+  __syncthreads();
+  int* err = &c.st->stage_err;
+  if (tid >= NT) {
+    if (tid == NT)
+      staged_loop_produce<CFG, double, CI>(a, c.tiles + me.t0, count, pipe, staged_smem, err);
+    return;
+  }
+
+  double* rs = reinterpret_cast<double*>(staged_smem + STAGES_BYTES);
+  auto r_at = [&](int g) -> double& { return RS ? rs[g - me.g0] : c.r[g]; };
+  const uint64_t keep = l2_policy_keep();
+  const unsigned long long G = gridDim.x;
+
+  // Init: r = p = b, x = 0, rnorm0 = b.b.  Barrier epochs: 1 for the init,
+  // 3j+2, 3j+3, 3j+4 for phases A, B, C of iteration j.
+  double acc = 0.0;
+  for (int g = me.g0 + tid; g < me.g1; g += NT) {
+    const double bi = c.b[g];
+    r_at(g) = bi;
+    st_pol(c.p + g, bi, keep);
+    st_pol(c.x + g, 0.0, keep);
+    acc += bi * bi;
+  }
+  double rnorm0 = 0.0;
+  bool ok = coop_grid_sum<NT>(acc, c.partials2, c.bar, G, err, gs, &rnorm0);
+  if (tid == 0) {
+    sv.rtol2 = *static_cast<volatile double*>(&c.st->rtol2);
+    sv.kmax = *static_cast<volatile int*>(&c.st->kmax);
+    sv.rnorm0 = sv.rnorm_old = sv.rnorm_new = rnorm0;
+    sv.alpha = sv.beta = sv.pdoty = 0.0;
+    sv.k = 0;
+    sv.status = SPMV_SUCCESS;
+    sv.go = ok && sv.kmax > 0 && rnorm0 > 0.0 && isfinite(rnorm0);
+  }
+  named_sync(1, NT);
+  int k = 0;
+  while (sv.go) {
+    const unsigned long long e = 3ull * unsigned(k);
+    // A: y = A p, p.y.
+    acc = cg_fused_product<CFG, U, CI>(a, count, uint64_t(k) * uint64_t(count), pipe,
+                                       staged_smem, err, c.y, c.p);
+    double pdoty = 0.0;
+    if (!coop_grid_sum<NT>(acc, c.partials, c.bar, (e + 2) * G, err, gs, &pdoty)) {
+      ok = false;
+      break;
+    }
+    const bool broke = pdoty == 0.0 || !isfinite(pdoty);
+    const double alpha = sv.rnorm_old / pdoty;
+
+    // B: r -= alpha y, x += alpha p, r.r (skipped after a breakdown); V rows
+    // per thread in flight (r is read when used), as many as the shape's
+    // registers hold without spilling.
+    constexpr int V = CFG::MINB > 1 ? 4 : 2;
+    acc = 0.0;
+    if (!broke) {
+      for (int g0 = me.g0 + tid; g0 < me.g1; g0 += V * NT) {
+        double yv[V], pv[V], xv[V];
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+          const int g = g0 + u * NT;
+          if (g < me.g1) {
+            yv[u] = ld_pol(c.y + g, keep);
+            pv[u] = ld_pol(c.p + g, keep);
+            xv[u] = ld_pol(c.x + g, keep);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+          const int g = g0 + u * NT;
+          if (g < me.g1) {
+            const double ri = r_at(g) - alpha * yv[u];
+            r_at(g) = ri;
+            st_pol(c.x + g, xv[u] + alpha * pv[u], keep);
+            acc += ri * ri;
+          }
+        }
+      }
+    }
+    double rr = 0.0;
+    if (!coop_grid_sum<NT>(acc, c.partials2, c.bar, (e + 3) * G, err, gs, &rr)) {
+      ok = false;
+      break;
+    }
+    // beta, the count and the convergence test (one thread; every CTA
+    // computes the same from the same totals).
+    if (tid == 0) {
+      sv.k = k + 1;
+      sv.pdoty = pdoty;
+      sv.alpha = alpha;
+      if (broke) {
+        sv.status = SPMV_ERROR_BREAKDOWN;
+        sv.go = false;
+      } else {
+        sv.rnorm_new = rr;
+        sv.beta = rr / sv.rnorm_old;
+        sv.rnorm_old = rr;
+        const bool converged = rr / sv.rnorm0 < sv.rtol2;
+        sv.go = !converged && k + 1 < sv.kmax;
+      }
+    }
+    named_sync(1, NT);
+    k += 1;
+    if (!sv.go) break;
+
+    // C: p = p beta + r.
+    const double beta = sv.beta;
+    for (int g0 = me.g0 + tid; g0 < me.g1; g0 += V * NT) {
+      double pv[V];
+#pragma unroll
+      for (int u = 0; u < V; ++u) {
+        const int g = g0 + u * NT;
+        if (g < me.g1) pv[u] = ld_pol(c.p + g, keep);
+      }
+#pragma unroll
+      for (int u = 0; u < V; ++u) {
+        const int g = g0 + u * NT;
+        if (g < me.g1) st_pol(c.p + g, pv[u] * beta + r_at(g), keep);
+      }
+    }
+    if (!coop_grid_barrier<NT>(c.bar, (e + 4) * G, err, gs)) {
+      ok = false;
+      break;
+    }
+  }
+  if (tid == 0) {
+    pipe.stop = 1;
+    if (ok && blockIdx.x == 0) {
+      CgState* st = c.st;
+      st->rnorm0 = sv.rnorm0;
+      st->rnorm_old = sv.rnorm_old;
+      st->rnorm_new = sv.rnorm_new;
+      st->alpha = sv.alpha;
+      st->beta = sv.beta;
+      st->pdoty = sv.pdoty;
+      st->k = sv.k;
+      st->status = sv.status;
+    }
+  }
+}
+
+using FusedFn = void (*)(SpmvArgs, CgPtrs, const FusedCta*);
+
+// Fused shapes: one CTA per SM (28 consumer warps, 6 stages) or two
+// (12 consumer warps, 3 stages each), the rest of shared memory holding r;
+// with r in global memory, two CTAs of 6 stages (the stage bytes per SM of
+// the graph form's product).
+using CgFusedOne = StagedCfg<28, 6, 16384>;
+using CgFusedTwo = StagedCfg<12, 3, 16384, 2>;
+using CgFusedTwoDeep = StagedCfg<12, 6, 16384, 2>;
+
+template <class CFG, bool D16, bool RS>
+FusedFn fused_fn_u(int U) {
+  switch (staged_width(U)) {
+    case 8: return cg_fused<CFG, 8, D16, RS>;
+    case 7: return cg_fused<CFG, 7, D16, RS>;
+    case 5: return cg_fused<CFG, 5, D16, RS>;
+    default: return cg_fused<CFG, 4, D16, RS>;
+  }
+}
+
+template <class CFG, bool RS>
+FusedFn fused_fn(const SolverProduct& sp) {
+  return sp.d16 ? fused_fn_u<CFG, true, RS>(sp.w) : fused_fn_u<CFG, false, RS>(sp.w);
 }
 
 using K1Fn = void (*)(SpmvArgs, CgPtrs, cudaGraphConditionalHandle);
@@ -293,6 +539,8 @@ CgPtrs cg_ptrs(CgWorkspace& w) {
   c.n = w.n;
   c.tiles = w.tiles;
   c.ntiles = w.ntiles;
+  c.bar = w.bar.as<unsigned long long>();
+  c.partials2 = w.partials2.as<double>();
   return c;
 }
 
@@ -383,6 +631,207 @@ void build_graph(spmv_matrix A, CgWorkspace& w) {
   SPMVB_CUDA(cudaGraphInstantiate(&w.exec, w.graph, 0));
 }
 
+// Fused solve plans.  The tiles are split into `grid` contiguous runs of
+// about n / grid rows each (tile starts are row boundaries, so each run
+// covers a contiguous range of global rows); returns the longest run.
+int64_t fused_ctas(spmv_matrix A, const DevCsr::StagedTable& t, int grid,
+                   std::vector<FusedCta>& out) {
+  const std::vector<int64_t>& ranges = A->row_map->ranges;
+  const int T = t.ntiles;
+  const int64_t n = ranges.back();
+  std::vector<int64_t> start(size_t(T) + 1);
+  for (int k = 0; k < T; ++k) {
+    const DevCsr::StagedTable::Rows& r = t.rows[size_t(k)];
+    start[size_t(k)] =
+        std::min<int64_t>(ranges[size_t(r.rank)] + int64_t(r.s0) * 32, ranges[size_t(r.rank) + 1]);
+  }
+  start[size_t(T)] = n;
+  out.assign(size_t(grid), FusedCta{});
+  int kb = 0;
+  int64_t longest = 0;
+  for (int b = 0; b < grid; ++b) {
+    const int64_t target = n * (b + 1) / grid;
+    const int ke = b + 1 == grid
+                       ? T
+                       : int(std::lower_bound(start.begin() + kb, start.end(), target) -
+                             start.begin());
+    out[size_t(b)] = {kb, ke, int32_t(start[size_t(kb)]), int32_t(start[size_t(ke)])};
+    longest = std::max(longest, start[size_t(ke)] - start[size_t(kb)]);
+    kb = ke;
+  }
+  return longest;
+}
+
+struct FusedPlan {
+  const void* fn = nullptr;
+  int grid = 0, block = 0, smem = 0;
+  int cps = 0;      // CTAs per SM
+  bool rs = false;  // r in shared memory
+  std::vector<FusedCta> ctas;
+};
+
+// A plan for shape CFG (CFG::MINB CTAs per SM), r in shared memory (RS) or
+// global memory; false when it does not fit.
+template <class CFG, bool RS>
+bool plan_fused(spmv_matrix A, const SolverProduct& sp, FusedPlan& plan) {
+  const int cps = CFG::MINB;
+  const bool rs = RS;
+  const int eb = 8 + (sp.d16 ? 2 : 4);
+  static_assert(CFG::max_entries(10) == SolverStaged::max_entries(10) &&
+                    CFG::max_entries(12) == SolverStaged::max_entries(12),
+                "fused shapes use the solver product's tiles");
+  const DevCsr::StagedTable& t = cg_tiles(A, sp);
+  if (!t.ok) return false;
+  spmv_comm comm = A->comm;
+  const int grid = std::max(1, comm->num_sms) * cps;
+  std::vector<FusedCta> ctas;
+  const int64_t longest = fused_ctas(A, t, grid, ctas);
+  const int64_t smem = CFG::smem_bytes(eb) + (rs ? (longest * 8 + 15) / 16 * 16 : 0);
+  const void* fn = (const void*)fused_fn<CFG, RS>(sp);
+  int optin = 0;
+  SPMVB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                    comm->device));
+  cudaFuncAttributes fa{};
+  SPMVB_CUDA(cudaFuncGetAttributes(&fa, fn));
+  if (smem + int64_t(fa.sharedSizeBytes) > optin) return false;
+  SPMVB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  int nb = 0;
+  SPMVB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, CFG::BS, size_t(smem)));
+  if (nb < cps) return false;
+  plan.fn = fn;
+  plan.grid = grid;
+  plan.block = CFG::BS;
+  plan.smem = int(smem);
+  plan.cps = cps;
+  plan.rs = rs;
+  plan.ctas = std::move(ctas);
+  return true;
+}
+
+void use_plan(CgWorkspace& w, FusedPlan& plan) {
+  w.fused = true;
+  w.fused_fn = plan.fn;
+  w.fused_grid = plan.grid;
+  w.fused_block = plan.block;
+  w.fused_smem = plan.smem;
+  w.fused_cps = plan.cps;
+  w.fused_rs = plan.rs;
+  w.ctas.reserve(sizeof(FusedCta) * plan.ctas.size());
+  SPMVB_CUDA(cudaMemcpy(w.ctas.ptr, plan.ctas.data(), sizeof(FusedCta) * plan.ctas.size(),
+                        cudaMemcpyHostToDevice));
+}
+
+// One solve as enqueued by cg_run (kmax, rtol^2 and the error flag first).
+void enqueue_solve(CgWorkspace& w, cudaStream_t s) {
+  CgState* st = w.state.as<CgState>();
+  static_assert(offsetof(CgState, stage_err) + sizeof(int) - offsetof(CgState, rtol2) == 32,
+                "rtol2 .. stage_err are one contiguous block");
+  SPMVB_CUDA(cudaMemcpyAsync(&st->rtol2, &w.host.rtol2, 32, cudaMemcpyHostToDevice, s));
+  if (w.fused) {
+    SPMVB_CUDA(cudaMemsetAsync(w.bar.ptr, 0, sizeof(unsigned long long), s));
+    CgPtrs c = cg_ptrs(w);
+    const FusedCta* ctas = w.ctas.as<FusedCta>();
+    void* args[] = {&w.fused_args, &c, &ctas};
+    SPMVB_CUDA(cudaLaunchCooperativeKernel(w.fused_fn, dim3(w.fused_grid), dim3(w.fused_block),
+                                           args, size_t(w.fused_smem), s));
+  } else {
+    SPMVB_CUDA(cudaGraphLaunch(w.exec, s));
+  }
+}
+
+__global__ void cg_fill(double* v, int64_t n, double value) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    v[i] = value;
+}
+
+// Device time of `its` iterations of the current form (b = 1, no
+// convergence test can pass), best of three.
+float time_iterations(CgWorkspace& w, cudaStream_t s, int its) {
+  w.host.kmax = its;
+  w.host.rtol2 = 0.0;
+  w.host.stage_err = 0;
+  cudaEvent_t e0, e1;
+  SPMVB_CUDA(cudaEventCreate(&e0));
+  SPMVB_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    SPMVB_CUDA(cudaEventRecord(e0, s));
+    enqueue_solve(w, s);
+    SPMVB_CUDA(cudaEventRecord(e1, s));
+    SPMVB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SPMVB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (rep > 0) best = std::min(best, ms);
+  }
+  SPMVB_CUDA(cudaEventDestroy(e0));
+  SPMVB_CUDA(cudaEventDestroy(e1));
+  SPMVB_CUDA(cudaMemcpy(&w.host, w.state.ptr, sizeof(CgState), cudaMemcpyDeviceToHost));
+  if (w.host.stage_err)
+    fail(SPMV_ERROR_CUDA, "spmv::cg - a bounded wait of the fused solve timed out");
+  return best;
+}
+
+// Chooses between the graph form and the fused plans that fit, by timing a
+// few iterations of each on b = 1: r in shared memory with one or two CTAs
+// per SM (when the CTAs' rows fit), and two CTAs per SM of deeper pipelines
+// with r in global memory.  SPMV_B200_CG_FUSED: "0" keeps the graph form;
+// "<cps>:<smem|global>" forces that plan (1:global is the one-CTA shape),
+// failing if it does not fit.
+void choose_form(spmv_matrix A, CgWorkspace& w) {
+  w.fused = false;
+  if (w.product.kind != ProductKind::Staged || w.n == 0) return;
+  const char* env = std::getenv("SPMV_B200_CG_FUSED");
+  const std::string mode = env ? env : "";
+  if (mode == "0") return;
+  spmv_comm comm = A->comm;
+  int coop = 0;
+  SPMVB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, comm->device));
+  if (!coop) return;
+  w.bar.reserve(sizeof(unsigned long long));
+  w.partials2.reserve(sizeof(double) * std::max(1, comm->num_sms) * 2);
+  w.fused_args = k1_args(A, w, w.product);
+
+  const SolverProduct& sp = w.product;
+  if (!mode.empty()) {
+    FusedPlan p;
+    bool fits = false;
+    if (mode == "1:smem") fits = plan_fused<CgFusedOne, true>(A, sp, p);
+    else if (mode == "2:smem") fits = plan_fused<CgFusedTwo, true>(A, sp, p);
+    else if (mode == "1:global") fits = plan_fused<CgFusedOne, false>(A, sp, p);
+    else if (mode == "2:global") fits = plan_fused<CgFusedTwoDeep, false>(A, sp, p);
+    require(fits, "spmv: SPMV_B200_CG_FUSED must be 0 or a fused plan that fits this matrix "
+                  "(1:smem, 2:smem, 1:global, 2:global)");
+    use_plan(w, p);
+    return;
+  }
+  std::vector<FusedPlan> plans;
+  {
+    FusedPlan p1, p2, p3;
+    if (plan_fused<CgFusedOne, true>(A, sp, p1)) plans.push_back(std::move(p1));
+    if (plan_fused<CgFusedTwo, true>(A, sp, p2)) plans.push_back(std::move(p2));
+    if (plan_fused<CgFusedTwoDeep, false>(A, sp, p3)) plans.push_back(std::move(p3));
+  }
+  if (plans.empty()) return;
+  cudaStream_t s = A->comm->stream;
+  const int its = 8;
+  SPMVB_CUDA(cudaDeviceSynchronize());
+  cg_fill<<<std::max(1, comm->num_sms) * 4, 256, 0, s>>>(w.b.as<double>(), w.n, 1.0);
+  SPMVB_CUDA(cudaGetLastError());
+  float best = time_iterations(w, s, its);
+  int pick = -1;
+  for (size_t i = 0; i < plans.size(); ++i) {
+    use_plan(w, plans[i]);
+    const float t = time_iterations(w, s, its);
+    if (t < best) {
+      best = t;
+      pick = int(i);
+    }
+  }
+  w.fused = false;
+  if (pick >= 0) use_plan(w, plans[size_t(pick)]);
+}
+
 }  // namespace
 
 void destroy_cg_workspace(CgWorkspace* w) { delete w; }
@@ -438,6 +887,7 @@ CgWorkspace& cg_workspace(spmv_matrix A) {
       ws.ntiles = t.ntiles;
     }
     build_graph(A, ws);
+    choose_form(A, ws);
     A->cg = std::move(w);
   }
   return *A->cg;
@@ -446,6 +896,16 @@ CgWorkspace& cg_workspace(spmv_matrix A) {
 SolverProduct cg_product(spmv_matrix A) {
   require(A->cg != nullptr, "spmv: spmv_cg has not run on this matrix");
   return A->cg->product;
+}
+
+CgForm cg_form(spmv_matrix A) {
+  require(A->cg != nullptr, "spmv: spmv_cg has not run on this matrix");
+  const CgWorkspace& w = *A->cg;
+  CgForm f;
+  f.fused = w.fused;
+  f.cps = w.fused ? w.fused_cps : 0;
+  f.rs = w.fused && w.fused_rs;
+  return f;
 }
 
 double* cg_rhs(spmv_matrix A) { return cg_workspace(A).b.as<double>(); }
@@ -457,12 +917,9 @@ void cg_run(spmv_matrix A, int max_its, double rtol, spmv_cg_info* info) {
   // kmax and rtol^2 for this solve (cg.cpp:49).
   w.host.kmax = max_its;
   w.host.rtol2 = rtol * rtol;
+  w.host.stage_err = 0;
   CgState* st = w.state.as<CgState>();
-  SPMVB_CUDA(cudaMemcpyAsync(&st->kmax, &w.host.kmax, sizeof(int),
-                             cudaMemcpyHostToDevice, s));
-  SPMVB_CUDA(cudaMemcpyAsync(&st->rtol2, &w.host.rtol2, sizeof(double),
-                             cudaMemcpyHostToDevice, s));
-  SPMVB_CUDA(cudaGraphLaunch(w.exec, s));
+  enqueue_solve(w, s);
   SPMVB_CUDA(cudaMemcpyAsync(&w.host, st, sizeof(CgState),
                              cudaMemcpyDeviceToHost, s));
   SPMVB_CUDA(cudaStreamSynchronize(s));

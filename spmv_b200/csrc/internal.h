@@ -241,6 +241,11 @@ struct DevCsr {
     bool built = false, ok = false;
     int ntiles = 0;
     DevBuf desc;
+    // Host copy of each tile's rank, first slice and slice count.
+    struct Rows {
+      int32_t rank, s0, nslices;
+    };
+    std::vector<Rows> rows;
   } staged[4];
   // Row statistics (over all ranks).
   double mean_row = 0;
@@ -361,6 +366,13 @@ SolverProduct choose_solver_product(spmv_matrix A, spmv_dtype dt, const void* x,
                                     bool xown_rows, const ProductLauncher& launch);
 // The products chosen by the built solver workspaces (fails if none).
 SolverProduct cg_product(spmv_matrix A);
+// How the built CG workspace runs a solve (fails if none).
+struct CgForm {
+  bool fused = false;
+  int cps = 0;
+  bool rs = false;
+};
+CgForm cg_form(spmv_matrix A);
 SolverProduct ir_product(spmv_matrix A, bool fp32);
 // Builds the SELL copies the solvers may time (when SELL is applicable).
 void prepare_solver_layouts(spmv_matrix A, bool fp32);

@@ -123,6 +123,7 @@ template <int KIND>
 __host__ __device__ constexpr int kind_bs() {
   return KIND == 2 ? SolverStaged::BS : 256;
 }
+
 template <typename T, int W, int KIND, bool D16, class F>
 __device__ __forceinline__ void rows_of(const SpmvArgs& a, const StagedDesc* tiles, int ntiles,
                                         int* err, F&& f) {
@@ -139,9 +140,8 @@ __device__ __forceinline__ void rows_of(const SpmvArgs& a, const StagedDesc* til
 // K1: y = A32 p (FP32 row sums), p.y accumulated in FP64.  !H: the same
 // kernel outside the graph (no loop condition), for timing candidates.
 template <int W, int KIND, bool D16, bool H>
-__global__ void __launch_bounds__(kind_bs<KIND>())
-    ir_spmv_dot(const __grid_constant__ SpmvArgs a, const IrPtrs c,
-                cudaGraphConditionalHandle h_loop) {
+__device__ __forceinline__ void ir_spmv_dot_body(const SpmvArgs& a, const IrPtrs& c,
+                                                 cudaGraphConditionalHandle h_loop) {
   constexpr int BS = kind_bs<KIND>();
   __shared__ double smem[32];
   if (H && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h_loop, 0u);
@@ -160,6 +160,21 @@ __global__ void __launch_bounds__(kind_bs<KIND>())
     if (total == 0.0 || !isfinite(total)) st->status = SPMV_ERROR_BREAKDOWN;
     st->alpha = st->rr / total;
   }
+}
+
+// Launch bounds: the vector and SELL forms keep the compiler's own register
+// choice; the staged form is compiled for its 3 resident CTAs per SM.
+template <int W, int KIND, bool D16, bool H>
+__global__ void __launch_bounds__(256)
+    ir_spmv_dot(const __grid_constant__ SpmvArgs a, const IrPtrs c,
+                cudaGraphConditionalHandle h_loop) {
+  ir_spmv_dot_body<W, KIND, D16, H>(a, c, h_loop);
+}
+template <int W, bool D16, bool H>
+__global__ void __launch_bounds__(SolverStaged::BS, SolverStaged::MINB)
+    ir_spmv_dot_staged(const __grid_constant__ SpmvArgs a, const IrPtrs c,
+                       cudaGraphConditionalHandle h_loop) {
+  ir_spmv_dot_body<W, 2, D16, H>(a, c, h_loop);
 }
 
 // K2: r -= alpha y, r.r; decides whether to refine.  (The correction
@@ -213,8 +228,7 @@ __global__ void __launch_bounds__(EW) ir_fold(const IrPtrs c) {
 
 // Refinement 2: r64 = b - A x in FP64, and its norm.
 template <int W, int KIND, bool D16>
-__global__ void __launch_bounds__(kind_bs<KIND>())
-    ir_residual(const __grid_constant__ SpmvArgs a, const IrPtrs c) {
+__device__ __forceinline__ void ir_residual_body(const SpmvArgs& a, const IrPtrs& c) {
   constexpr int BS = kind_bs<KIND>();
   __shared__ double smem[32];
   double acc = 0.0;
@@ -235,6 +249,17 @@ __global__ void __launch_bounds__(kind_bs<KIND>())
     if (total / st->rr0 < st->rtol2) st->converged = 1;
     if (!isfinite(total)) st->status = SPMV_ERROR_BREAKDOWN;
   }
+}
+
+template <int W, int KIND, bool D16>
+__global__ void __launch_bounds__(256)
+    ir_residual(const __grid_constant__ SpmvArgs a, const IrPtrs c) {
+  ir_residual_body<W, KIND, D16>(a, c);
+}
+template <int W, bool D16>
+__global__ void __launch_bounds__(SolverStaged::BS, SolverStaged::MINB)
+    ir_residual_staged(const __grid_constant__ SpmvArgs a, const IrPtrs c) {
+  ir_residual_body<W, 2, D16>(a, c);
 }
 
 // Refinement 3: r = fl32(r64); r.r and r.p (FP64) for beta and the
@@ -300,41 +325,43 @@ using KR = void (*)(SpmvArgs, IrPtrs);
 // lane (1..16), staged gathers in flight per lane (4 or 8).
 template <int KIND, bool D16, bool H>
 K1 pick_k1(int W) {
-  if (KIND == 2) {
+  if constexpr (KIND == 2) {
     switch (staged_width(W)) {
-      case 8: return ir_spmv_dot<8, KIND, D16, H>;
-      case 7: return ir_spmv_dot<7, KIND, D16, H>;
-      case 5: return ir_spmv_dot<5, KIND, D16, H>;
-      default: return ir_spmv_dot<4, KIND, D16, H>;
+      case 8: return ir_spmv_dot_staged<8, D16, H>;
+      case 7: return ir_spmv_dot_staged<7, D16, H>;
+      case 5: return ir_spmv_dot_staged<5, D16, H>;
+      default: return ir_spmv_dot_staged<4, D16, H>;
     }
-  }
-  switch (W) {
-    case 1: return ir_spmv_dot<1, KIND, D16, H>;
-    case 2: return ir_spmv_dot<2, KIND, D16, H>;
-    case 4: return ir_spmv_dot<4, KIND, D16, H>;
-    case 8: return ir_spmv_dot<8, KIND, D16, H>;
-    case 16: return ir_spmv_dot<16, KIND, D16, H>;
-    case 32: if (KIND == 0) return ir_spmv_dot<32, KIND, D16, H>;
+  } else {
+    switch (W) {
+      case 1: return ir_spmv_dot<1, KIND, D16, H>;
+      case 2: return ir_spmv_dot<2, KIND, D16, H>;
+      case 4: return ir_spmv_dot<4, KIND, D16, H>;
+      case 8: return ir_spmv_dot<8, KIND, D16, H>;
+      case 16: return ir_spmv_dot<16, KIND, D16, H>;
+      case 32: if (KIND == 0) return ir_spmv_dot<32, KIND, D16, H>;
+    }
   }
   fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: unsupported product width");
 }
 template <int KIND, bool D16>
 KR pick_kr(int W) {
-  if (KIND == 2) {
+  if constexpr (KIND == 2) {
     switch (staged_width(W)) {
-      case 8: return ir_residual<8, KIND, D16>;
-      case 7: return ir_residual<7, KIND, D16>;
-      case 5: return ir_residual<5, KIND, D16>;
-      default: return ir_residual<4, KIND, D16>;
+      case 8: return ir_residual_staged<8, D16>;
+      case 7: return ir_residual_staged<7, D16>;
+      case 5: return ir_residual_staged<5, D16>;
+      default: return ir_residual_staged<4, D16>;
     }
-  }
-  switch (W) {
-    case 1: return ir_residual<1, KIND, D16>;
-    case 2: return ir_residual<2, KIND, D16>;
-    case 4: return ir_residual<4, KIND, D16>;
-    case 8: return ir_residual<8, KIND, D16>;
-    case 16: return ir_residual<16, KIND, D16>;
-    case 32: if (KIND == 0) return ir_residual<32, KIND, D16>;
+  } else {
+    switch (W) {
+      case 1: return ir_residual<1, KIND, D16>;
+      case 2: return ir_residual<2, KIND, D16>;
+      case 4: return ir_residual<4, KIND, D16>;
+      case 8: return ir_residual<8, KIND, D16>;
+      case 16: return ir_residual<16, KIND, D16>;
+      case 32: if (KIND == 0) return ir_residual<32, KIND, D16>;
+    }
   }
   fail(SPMV_ERROR_INVALID_ARGUMENT, "spmv: unsupported product width");
 }

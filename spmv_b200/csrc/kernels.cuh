@@ -294,4 +294,93 @@ __device__ __forceinline__ bool grid_sum2(double a, double b, double* partials,
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// Grid barrier and grid sum for cooperative launches (every CTA resident),
+// over the first NT threads of each CTA (named barrier 1; the CTA's other
+// warps do not take part).  `count` is zero at launch; the e-th barrier of
+// the launch waits for count = e * gridDim.x.  Waits are bounded: a barrier
+// that does not complete, or sees *err raised, raises *err and returns false
+// (CTAs that have already passed fail at their next barrier).
+__device__ __forceinline__ void named_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// One thread per CTA, after a CTA barrier: arrival is a release (the CTA's
+// writes before the barrier are visible to any CTA that sees the count),
+// the wait an acquire.
+__device__ __forceinline__ bool grid_arrive_wait(unsigned long long* count,
+                                                 unsigned long long target, int* err) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(count), "l"(1ull) : "memory");
+  for (uint32_t i = 0; i < (1u << 23); ++i) {
+    unsigned long long c;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(c) : "l"(count) : "memory");
+    if (c >= target) return true;
+    if (*static_cast<volatile int*>(err)) return false;
+    if (i >= 64) __nanosleep(32);
+  }
+  atomicExch(err, 1);
+  return false;
+}
+
+template <int NT>
+struct GridSum {
+  double red[NT / 32];
+  double total;
+  int ok;
+};
+
+// Barrier only.  All NT threads call it; returns the same verdict in all.
+template <int NT>
+__device__ __forceinline__ bool coop_grid_barrier(unsigned long long* count,
+                                                  unsigned long long target, int* err,
+                                                  GridSum<NT>& s) {
+  named_sync(1, NT);
+  if (threadIdx.x == 0) s.ok = grid_arrive_wait(count, target, err);
+  named_sync(1, NT);
+  return s.ok != 0;
+}
+
+// Warp sums of v into s.red (then a barrier of the NT threads).
+template <int NT>
+__device__ __forceinline__ void warp_partials(double v, GridSum<NT>& s) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) s.red[threadIdx.x >> 5] = v;
+  named_sync(1, NT);
+}
+
+// s.red summed in warp order (one thread).
+template <int NT>
+__device__ __forceinline__ double sum_partials(const GridSum<NT>& s) {
+  double t = 0.0;
+#pragma unroll 4
+  for (int w = 0; w < NT / 32; ++w) t += s.red[w];
+  return t;
+}
+
+// Sum of v over the NT threads of every CTA.  Each CTA publishes its partial
+// (warp sums, then warps in index order) in parts[blockIdx.x]; after the
+// barrier every CTA reads all partials at once (thread i takes partials i,
+// i + NT, ...) and reduces them in the same fixed order, so all CTAs hold
+// the same total.
+template <int NT>
+__device__ __forceinline__ bool coop_grid_sum(double v, double* parts, unsigned long long* count,
+                                              unsigned long long target, int* err,
+                                              GridSum<NT>& s, double* total) {
+  warp_partials<NT>(v, s);
+  if (threadIdx.x == 0) {
+    __stcg(parts + blockIdx.x, sum_partials<NT>(s));
+    s.ok = grid_arrive_wait(count, target, err);
+  }
+  named_sync(1, NT);
+  if (!s.ok) return false;
+  double t = 0.0;
+  for (unsigned int i = threadIdx.x; i < gridDim.x; i += unsigned(NT)) t += __ldcg(parts + i);
+  warp_partials<NT>(t, s);
+  if (threadIdx.x == 0) s.total = sum_partials<NT>(s);
+  named_sync(1, NT);
+  *total = s.total;
+  return true;
+}
+
 }  // namespace spmvb

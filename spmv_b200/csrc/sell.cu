@@ -176,6 +176,8 @@ const DevCsr::StagedTable& staged_table(DevCsr& C, int entry_bytes, int max_entr
   t.ok = ok && !tiles.empty();
   if (!t.ok) return t;
   t.ntiles = int(tiles.size());
+  t.rows.reserve(tiles.size());
+  for (const StagedDesc& d : tiles) t.rows.push_back({d.rank, d.s0, d.nslices});
   t.desc.reserve(sizeof(StagedDesc) * tiles.size());
   SPMVB_CUDA(cudaMemcpy(t.desc.ptr, tiles.data(), sizeof(StagedDesc) * tiles.size(),
                         cudaMemcpyHostToDevice));
@@ -358,7 +360,7 @@ StagedShape staged_shape(const void* fn, int entry_bytes, int ntiles, int num_sm
 namespace {
 
 template <typename T, typename CI, int U>
-__global__ void __launch_bounds__(SolverStaged::BS)
+__global__ void __launch_bounds__(SolverStaged::BS, SolverStaged::MINB)
     spmv_staged_kernel(const __grid_constant__ SpmvArgs a, const StagedDesc* tiles, int ntiles,
                        int* err) {
   sell_staged_rows<SolverStaged, T, CI, U>(

@@ -38,12 +38,14 @@ constexpr int STAGED_HEADER_BYTES = 128;
 constexpr int STAGED_MAX_SLICES = 16;
 
 // Pipeline shape: NC consumer warps (+ one producer warp), STAGES tiles in
-// flight per CTA, DATA bytes of values + indices per tile.
-template <int NC_, int STAGES_, int DATA_>
+// flight per CTA, DATA bytes of values + indices per tile; MINB: CTAs per SM
+// a persistent kernel of this shape is compiled to fit (register bound).
+template <int NC_, int STAGES_, int DATA_, int MINB_ = 1>
 struct StagedCfg {
   static constexpr int NC = NC_;
   static constexpr int STAGES = STAGES_;
   static constexpr int DATA = DATA_;
+  static constexpr int MINB = MINB_;
   static constexpr int BS = 32 * (NC + 1);
   // Entries of one stage for `eb` bytes per entry (a multiple of 32).
   __host__ __device__ static constexpr int max_entries(int eb) { return (DATA / eb) / 32 * 32; }
@@ -57,7 +59,7 @@ struct StagedCfg {
 // The shape the solvers' products use: 12 consumer warps, 4 stages of 16 KB
 // (3 CTAs per SM), measured best of the shapes tried on the 7-point stencil
 // in FP64 and FP32.
-using SolverStaged = StagedCfg<12, 4, 16384>;
+using SolverStaged = StagedCfg<12, 4, 16384, 3>;
 
 // Descriptor of one tile (host-built, 128 bytes, copied as the stage's
 // header): slices [s0, s0 + nslices) of rank `rank`, whose entries start at
@@ -123,6 +125,100 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
+// The consumer side of one landed stage (header + values + indices at
+// `stage`): warp `warp` sums its share of the tile's slices (dealt round
+// robin, continuing from q0 = slices dealt before this tile; q0 is
+// advanced), one lane per row, entries in storage order, and calls
+// f(P, row, sum) for each row that exists.
+template <class CFG, typename T, typename CI, int U, class F, class G>
+__device__ __forceinline__ void staged_tile_rows(const SpmvArgs& a,
+                                                 const unsigned char* stage, int warp,
+                                                 int lane, int& q0, F&& f, const G& gx) {
+  constexpr int NC = CFG::NC;
+  constexpr int MAXE = CFG::max_entries(int(sizeof(T) + sizeof(CI)));
+  const StagedDesc* h = reinterpret_cast<const StagedDesc*>(stage);
+  const T* sv = reinterpret_cast<const T*>(stage + STAGED_HEADER_BYTES);
+  const CI* sc = reinterpret_cast<const CI*>(stage + STAGED_HEADER_BYTES + MAXE * int(sizeof(T)));
+  const PartArg& P = a.part[h->rank];
+  const int ns = h->nslices;
+  const int j0 = ((warp - q0) % NC + NC) % NC;
+  q0 += ns;
+  for (int j = j0; j < ns; j += NC) {
+    const int o = h->off[j];
+    const int w = (h->off[j + 1] - o) >> 5;
+    const int row = (h->s0 + j) * 32 + lane;
+    const int g = P.row0 + row;
+    T sum = T(0);
+    if (w == U) {
+      // The slice's rows in one chunk: no slot masks.  A padding entry
+      // gathers x[0] (in bounds in every layout; the value is not used).
+      T v[U], xv[U];
+      bool ok[U];
+      int c[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int idx = o + u * 32 + lane;
+        const int ci = int(sc[idx]);
+        v[u] = sv[idx];
+        ok[u] = sizeof(CI) == 2 ? ci != -32768 : ci >= 0;
+        c[u] = ok[u] ? (sizeof(CI) == 2 ? g + ci : ci) : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) xv[u] = gx(P, c[u]);
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (ok[u]) sum += v[u] * xv[u];
+      if (row < P.nrows) f(P, row, sum);
+      continue;
+    }
+    for (int k0 = 0; k0 < w; k0 += U) {
+      T v[U], xv[U];
+      bool ok[U];
+      int c[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const bool in = k0 + u < w;
+        const int idx = o + (k0 + u) * 32 + lane;
+        const int ci = in ? int(sc[idx]) : 0;
+        v[u] = in ? sv[idx] : T(0);
+        if (sizeof(CI) == 2) {
+          ok[u] = in && ci != -32768;
+          c[u] = g + ci;
+        } else {
+          ok[u] = in && ci >= 0;
+          c[u] = ci;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) xv[u] = ok[u] ? gx(P, c[u]) : T(0);
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (ok[u]) sum += v[u] * xv[u];
+    }
+    if (row < P.nrows) f(P, row, sum);
+  }
+}
+
+// Issues the bulk copies of one tile (descriptor d, whose rank, first
+// entry and entry count the caller has loaded as rk, e0, n) into `stage`,
+// completing on `full`.
+template <class CFG, typename T, typename CI>
+__device__ __forceinline__ void staged_issue(const SpmvArgs& a, const StagedDesc* d, int rk,
+                                             int e0, uint32_t n, unsigned char* stage,
+                                             uint64_t* full, uint64_t policy) {
+  constexpr int EB = int(sizeof(T) + sizeof(CI));
+  constexpr int MAXE = CFG::max_entries(EB);
+  const PartArg& P = a.part[rk];
+  mbar_arrive_expect_tx(full, STAGED_HEADER_BYTES + n * uint32_t(EB));
+  bulk_g2s(stage, d, STAGED_HEADER_BYTES, full, policy);
+  if (n > 0) {
+    bulk_g2s(stage + STAGED_HEADER_BYTES, static_cast<const T*>(P.vals) + e0,
+             n * uint32_t(sizeof(T)), full, policy);
+    bulk_g2s(stage + STAGED_HEADER_BYTES + MAXE * int(sizeof(T)),
+             reinterpret_cast<const CI*>(P.cols) + e0, n * uint32_t(sizeof(CI)), full, policy);
+  }
+}
+
 // Traversal.  CI: int32_t (columns, -1 = padding) or int16_t (offsets from
 // the global row g = row0 + row, -32768 = padding).  U: gathers in flight
 // per lane; gx(P, c): the gathered vector (XGather: the PartArg's x).
@@ -134,9 +230,7 @@ __device__ __forceinline__ void sell_staged_rows(const SpmvArgs& a,
                                                  int ntiles, int* err, F&& f, const G& gx) {
   constexpr int STAGED_STAGES = CFG::STAGES;
   constexpr int STAGED_CONSUMERS = CFG::NC;
-  constexpr int EB = int(sizeof(T) + sizeof(CI));
-  constexpr int MAXE = CFG::max_entries(EB);
-  constexpr int STAGE = CFG::stage_bytes(EB);
+  constexpr int STAGE = CFG::stage_bytes(int(sizeof(T) + sizeof(CI)));
   extern __shared__ __align__(128) unsigned char staged_smem[];
   __shared__ __align__(8) uint64_t full[STAGED_STAGES], empty[STAGED_STAGES];
 
@@ -145,16 +239,6 @@ __device__ __forceinline__ void sell_staged_rows(const SpmvArgs& a,
   const int count = int(blockIdx.x) < ntiles
                         ? (ntiles - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x)
                         : 0;
-  auto header = [&](int st) {
-    return reinterpret_cast<const StagedDesc*>(staged_smem + st * STAGE);
-  };
-  auto stage_vals = [&](int st) {
-    return reinterpret_cast<T*>(staged_smem + st * STAGE + STAGED_HEADER_BYTES);
-  };
-  auto stage_cols = [&](int st) {
-    return reinterpret_cast<CI*>(staged_smem + st * STAGE + STAGED_HEADER_BYTES +
-                                 MAXE * int(sizeof(T)));
-  };
 
   if (tid == 0) {
     for (int s = 0; s < STAGED_STAGES; ++s) {
@@ -189,17 +273,8 @@ __device__ __forceinline__ void sell_staged_rows(const SpmvArgs& a,
           failed = true;
           break;
         }
-        const PartArg& P = a.part[cur.x];
-        const uint32_t n = uint32_t(cur.z);
-        mbar_arrive_expect_tx(&full[st], STAGED_HEADER_BYTES + n * uint32_t(EB));
-        bulk_g2s(staged_smem + st * STAGE, tiles + int(blockIdx.x) + i * int(gridDim.x),
-                 STAGED_HEADER_BYTES, &full[st], stream);
-        if (n > 0) {
-          bulk_g2s(stage_vals(st), static_cast<const T*>(P.vals) + cur.y,
-                   n * uint32_t(sizeof(T)), &full[st], stream);
-          bulk_g2s(stage_cols(st), reinterpret_cast<const CI*>(P.cols) + cur.y,
-                   n * uint32_t(sizeof(CI)), &full[st], stream);
-        }
+        staged_issue<CFG, T, CI>(a, tiles + int(blockIdx.x) + i * int(gridDim.x), cur.x, cur.y,
+                                 uint32_t(cur.z), staged_smem + st * STAGE, &full[st], stream);
         issued = i + 1;
       }
       if (failed) {
@@ -222,47 +297,105 @@ __device__ __forceinline__ void sell_staged_rows(const SpmvArgs& a,
       if (err && lane == 0) atomicExch(err, 1);
       break;
     }
-    const StagedDesc* h = header(st);
-    const PartArg& P = a.part[h->rank];
-    const T* sv = stage_vals(st);
-    const CI* sc = stage_cols(st);
-    const int ns = h->nslices;
-    const int j0 = ((warp - q0) % STAGED_CONSUMERS + STAGED_CONSUMERS) % STAGED_CONSUMERS;
-    q0 += ns;
-    for (int j = j0; j < ns; j += STAGED_CONSUMERS) {
-      const int o = h->off[j];
-      const int w = (h->off[j + 1] - o) >> 5;
-      const int row = (h->s0 + j) * 32 + lane;
-      const int g = P.row0 + row;
-      T sum = T(0);
-      for (int k0 = 0; k0 < w; k0 += U) {
-        T v[U], xv[U];
-        bool ok[U];
-        int c[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const bool in = k0 + u < w;
-          const int idx = o + (k0 + u) * 32 + lane;
-          const int ci = in ? int(sc[idx]) : 0;
-          v[u] = in ? sv[idx] : T(0);
-          if (sizeof(CI) == 2) {
-            ok[u] = in && ci != -32768;
-            c[u] = g + ci;
-          } else {
-            ok[u] = in && ci >= 0;
-            c[u] = ci;
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) xv[u] = ok[u] ? gx(P, c[u]) : T(0);
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-          if (ok[u]) sum += v[u] * xv[u];
-      }
-      if (row < P.nrows) f(P, row, sum);
-    }
+    staged_tile_rows<CFG, T, CI, U>(a, staged_smem + st * STAGE, warp, lane, q0, f, gx);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[st]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Multi-pass form, for a persistent solver kernel that traverses the same
+// tiles once per iteration.  The CTA's tiles are tiles[0, count); the
+// producer streams them pass after pass (tile sequence number q, tile
+// q % count, stage q % STAGES) until the consumers raise `stop`, so the next
+// pass's first tiles land while the consumers do other work between passes.
+template <class CFG>
+struct StagedLoop {
+  uint64_t full[CFG::STAGES], empty[CFG::STAGES];
+  volatile int stop;
+};
+
+// Thread 0; the caller synchronises the CTA before the pipeline starts.
+template <class CFG>
+__device__ __forceinline__ void staged_loop_init(StagedLoop<CFG>& L) {
+  for (int s = 0; s < CFG::STAGES; ++s) {
+    mbar_init(&L.full[s], 1);
+    mbar_init(&L.empty[s], CFG::NC);
+  }
+  L.stop = 0;
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Waits for phase `parity` of `bar` unless `stop` is raised first.
+// Returns 0 (phase complete), 1 (stopped) or 2 (gave up: bounded).
+__device__ __forceinline__ int mbar_wait_or_stop(uint64_t* bar, uint32_t parity,
+                                                 const volatile int* stop) {
+  for (uint32_t i = 0; i < (1u << 22); ++i) {
+    if (mbar_try_wait(bar, parity)) return 0;
+    if (*stop) return 1;
+  }
+  return 2;
+}
+
+// Producer: one lane.  On stop (or a wait that gave up, which also sets
+// *err) it waits, bounded, for its copies still in flight and returns.
+template <class CFG, typename T, typename CI>
+__device__ __forceinline__ void staged_loop_produce(const SpmvArgs& a,
+                                                    const StagedDesc* __restrict__ tiles,
+                                                    int count, StagedLoop<CFG>& L,
+                                                    unsigned char* smem, int* err) {
+  constexpr int S = CFG::STAGES;
+  constexpr int STAGE = CFG::stage_bytes(int(sizeof(T) + sizeof(CI)));
+  if (count <= 0) return;
+  const uint64_t stream = l2_policy_stream();
+  uint64_t issued = 0;
+  int4 nxt = make_int4(__ldg(&tiles[0].rank), __ldg(&tiles[0].e0), __ldg(&tiles[0].n), 0);
+  int inext = 0;
+  for (uint64_t q = 0;; ++q) {
+    const int st = int(q % S);
+    const int i = inext;
+    const int4 cur = nxt;
+    inext = i + 1 == count ? 0 : i + 1;
+    {
+      const StagedDesc* d = tiles + inext;
+      nxt = make_int4(__ldg(&d->rank), __ldg(&d->e0), __ldg(&d->n), 0);
+    }
+    if (q >= uint64_t(S)) {
+      const int w = mbar_wait_or_stop(&L.empty[st], uint32_t(q / S - 1) & 1u, &L.stop);
+      if (w == 2 && err) atomicExch(err, 1);
+      if (w != 0) break;
+    }
+    if (L.stop) break;
+    staged_issue<CFG, T, CI>(a, tiles + i, cur.x, cur.y, uint32_t(cur.z), smem + st * STAGE,
+                             &L.full[st], stream);
+    issued = q + 1;
+  }
+  for (uint64_t q = issued > uint64_t(S) ? issued - S : 0; q < issued; ++q)
+    mbar_wait_bounded(&L.full[q % S], uint32_t(q / S) & 1u);
+}
+
+// Consumers (warps 0 .. NC-1): one pass over the CTA's tiles, whose first
+// tile has sequence number q_base.  A stage that does not land within the
+// bound sets *err and ends this warp's pass.
+template <class CFG, typename T, typename CI, int U, class F, class G>
+__device__ __forceinline__ void staged_loop_consume(const SpmvArgs& a, int count, uint64_t q_base,
+                                                    StagedLoop<CFG>& L,
+                                                    const unsigned char* smem, int* err, F&& f,
+                                                    const G& gx) {
+  constexpr int S = CFG::STAGES;
+  constexpr int STAGE = CFG::stage_bytes(int(sizeof(T) + sizeof(CI)));
+  const int warp = int(threadIdx.x) >> 5, lane = int(threadIdx.x) & 31;
+  int q0 = 0;
+  for (int i = 0; i < count; ++i) {
+    const uint64_t q = q_base + uint64_t(i);
+    const int st = int(q % S);
+    if (!mbar_wait_bounded(&L.full[st], uint32_t(q / S) & 1u)) {
+      if (err && lane == 0) atomicExch(err, 1);
+      return;
+    }
+    staged_tile_rows<CFG, T, CI, U>(a, smem + st * STAGE, warp, lane, q0, f, gx);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&L.empty[st]);
   }
 }
 

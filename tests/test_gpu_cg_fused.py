@@ -1,0 +1,96 @@
+"""The fused CG solve (spmv::cg, cg.cpp:11-83, as one cooperative launch of
+persistent CTAs) against the graph form (three kernels per iteration) on the
+same matrix and staged product, for every fused plan: one or two CTAs per
+SM, the residual in shared or global memory.  Also the reference's edge
+cases through the fused form: zero right-hand side, the max_its cap,
+breakdown, and run-to-run reproducibility."""
+import numpy as np
+import pytest
+
+import spmv_b200 as S
+from spmv_b200 import gen
+from helpers import build
+
+pytestmark = pytest.mark.gpu
+
+PLANS = ["1:smem", "2:smem", "1:global", "2:global"]
+
+
+def setup(monkeypatch, plan, W, P, width=8):
+    monkeypatch.setenv("SPMV_B200_CG_FUSED", plan)
+    comm, cm, rm, M, D = build(W, P)
+    M.set_kernel("staged", width)
+    return comm, M, D
+
+
+def solve(monkeypatch, plan, W, P, width=8, max_its=10000):
+    comm, M, D = setup(monkeypatch, plan, W, P, width)
+    b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(P)]
+    x, k, info = S.cg(comm, M, b, max_its, W.rtol, info=True)
+    xg = np.concatenate([x[q][:D.local_sizes[q]] for q in range(P)])
+    return xg, k, info, M
+
+
+def true_relres(W, x):
+    return np.linalg.norm(W.b - W.A.scipy() @ x) / np.linalg.norm(W.b)
+
+
+@pytest.mark.parametrize("plan", PLANS)
+@pytest.mark.parametrize("cfg,scale,P,width", [("c2", 32, 8, 8), ("c2", 40, 3, 4),
+                                               ("c1", 64, 3, 4)])
+def test_fused_matches_graph_form(monkeypatch, cuda_device, plan, cfg, scale, P, width):
+    """Same per-element arithmetic as the graph form; only the grouping of
+    the two dot products' partial sums differs."""
+    W = gen.workload(cfg, scale)
+    x0, k0, i0, M0 = solve(monkeypatch, "0", W, P, width)
+    assert M0.cg_form() == ("graph", 0, None)
+    x1, k1, i1, M1 = solve(monkeypatch, plan, W, P, width)
+    cps, where = plan.split(":")
+    assert M1.cg_form() == ("fused", int(cps), where)
+    assert M1.solver_product("cg")[0] == "staged"
+    assert i1.status == 0 and i0.status == 0
+    assert abs(k1 - k0) <= 2, (k0, k1)
+    assert np.linalg.norm(x1 - x0) <= 1e-9 * np.linalg.norm(x0)
+    assert i1.rnorm / i1.rnorm0 < W.rtol ** 2
+    assert true_relres(W, x1) < 1.5 * W.rtol
+
+
+@pytest.mark.parametrize("plan", ["1:smem", "2:global"])
+def test_fused_repeats_and_caps(monkeypatch, cuda_device, plan):
+    W = gen.workload("c2", 32)
+    comm, M, D = setup(monkeypatch, plan, W, 8)
+    b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(8)]
+    x1, k1 = S.cg(comm, M, b, 10000, W.rtol)
+    x2, k2 = S.cg(comm, M, b, 10000, W.rtol)
+    assert M.cg_form()[0] == "fused"
+    assert k1 == k2 and all(np.array_equal(a, c) for a, c in zip(x1, x2))
+    x3, k3 = S.cg(comm, M, b, 7, W.rtol)  # max_its caps the count
+    assert k3 == 7
+    x4, k4 = S.cg(comm, M, [np.zeros(n) for n in D.local_sizes], 100, 1e-8)
+    assert k4 == 0 and all(np.all(v == 0) for v in x4)
+    # The workspace is reused after the zero right-hand side.
+    x5, k5 = S.cg(comm, M, b, 10000, W.rtol)
+    assert k5 == k1 and all(np.array_equal(a, c) for a, c in zip(x1, x5))
+
+
+@pytest.mark.parametrize("plan", ["1:smem", "2:global"])
+def test_fused_breakdown_is_reported(monkeypatch, cuda_device, plan):
+    W = gen.workload("c1", 16)
+    zero = gen.CSR(W.A.rowptr, W.A.cols, 0.0 * W.A.vals, W.A.ncols)
+    monkeypatch.setenv("SPMV_B200_CG_FUSED", plan)
+    comm, cm, rm, M, D = build(zero, 1)
+    M.set_kernel("staged", 4)
+    with pytest.raises(S.SpmvError) as e:
+        S.cg(comm, M, [W.b.copy()], 100, 1e-8)
+    assert e.value.status == 5 and "breakdown" in str(e.value)
+    assert M.cg_form()[0] == "fused"
+
+
+def test_fused_plan_that_does_not_fit_is_refused(monkeypatch, cuda_device):
+    W = gen.workload("c2", 16)
+    monkeypatch.setenv("SPMV_B200_CG_FUSED", "3:smem")
+    comm, cm, rm, M, D = build(W, 2)
+    M.set_kernel("staged", 8)
+    b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(2)]
+    with pytest.raises(S.SpmvError):
+        S.cg(comm, M, b, 100, W.rtol)
