@@ -54,8 +54,8 @@ typedef enum spmv_status {
 typedef enum spmv_dtype {
   SPMV_FLOAT64 = 0,
   SPMV_FLOAT32 = 1,
-  SPMV_COMPLEX64 = 2,  /* std::complex<float>  (not yet implemented) */
-  SPMV_COMPLEX128 = 3  /* std::complex<double> (not yet implemented) */
+  SPMV_COMPLEX64 = 2,  /* std::complex<float>: matrices, products, maps */
+  SPMV_COMPLEX128 = 3  /* std::complex<double>: matrices, products, maps */
 } spmv_dtype;
 
 typedef enum spmv_memory {
@@ -245,9 +245,11 @@ int spmv_matrix_set_values(spmv_matrix A, spmv_memory memory,
  *    kernel. */
 int spmv_matrix_mult_noalloc(spmv_matrix A, const void* const* x,
                              void* const* y);
-/* Kernel choice.  width: lanes per row for SPMV_KERNEL_VECTOR, or loads in
- * flight per lane for SPMV_KERNEL_SELL (1..32, power of two; 0 = from
- * statistics); block: threads per CTA (0 = default). */
+/* Kernel choice.  width: lanes per row for SPMV_KERNEL_VECTOR (1..32, a
+ * power of two), loads in flight per lane for SPMV_KERNEL_SELL (1..16, a
+ * power of two), gathers in flight per lane for SPMV_KERNEL_STAGED (4, 5, 7
+ * or 8; 5 and 7 suit stencils whose rows have exactly that many entries);
+ * 0 = from statistics; block: threads per CTA (0 = default). */
 int spmv_matrix_set_kernel(spmv_matrix A, spmv_kernel kernel, int width,
                            int block);
 int spmv_matrix_get_kernel(spmv_matrix A, spmv_kernel* kernel, int* width,

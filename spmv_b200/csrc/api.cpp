@@ -892,7 +892,8 @@ int spmv_matrix_set_kernel(spmv_matrix A, spmv_kernel kernel, int width,
                 kernel == SPMV_KERNEL_MERGE || kernel == SPMV_KERNEL_SELL ||
                 kernel == SPMV_KERNEL_STAGED,
             "spmv: unknown kernel");
-    require(width == 0 || (width >= 1 && width <= 32 && (width & (width - 1)) == 0),
+    require(kernel == SPMV_KERNEL_STAGED || width == 0 ||
+                (width >= 1 && width <= 32 && (width & (width - 1)) == 0),
             "spmv: width must be 0 or 1..32, a power of two");
     require(kernel != SPMV_KERNEL_SELL || width <= 16,
             "spmv: SELL width (loads in flight per lane) must be 1..16");

@@ -24,10 +24,12 @@
 // are summed in the same order as sell_for_rows, so results match that
 // traversal bit for bit.
 //
-// Every wait is bounded: a barrier that does not complete within the limit
-// sets *err and ends that warp's loop; the producer then waits (bounded
-// again) for the copies it issued, so no copy is left writing to the shared
-// memory of a finished CTA.
+// Every wait is bounded (2 s of global time): a barrier that does not
+// complete within the limit sets *err and ends that warp's loop; the
+// producer then waits (bounded again) for the copies it issued, so no copy
+// is left writing to the shared memory of a finished CTA.  Waiting warps
+// are suspended between probes, so they take no issue slots from the
+// warps that compute.
 #pragma once
 
 #include "spmv_kernel.cuh"
@@ -92,26 +94,51 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                : "memory");
 }
 
-// One probe of the barrier's phase (the instruction itself suspends for a
-// bounded, hardware-defined time); true once phase `parity` has completed.
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+// One probe of the barrier's phase: true once phase `parity` has completed.
+// The instruction may suspend the thread until the phase completes, for at
+// most `hint_ns` nanoseconds (0: the hardware's own limit).
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity,
+                                              uint32_t hint_ns = 0) {
   uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
+  if (hint_ns == 0) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+  }
   return ok != 0;
 }
 
-// Waits for phase `parity` of `bar`, giving up after a bounded number of
-// probes (seconds; a healthy pipeline needs microseconds).
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bound of every pipeline wait (a healthy pipeline waits microseconds).
+constexpr uint64_t STAGED_WAIT_LIMIT_NS = 2000000000ull;
+
+// Waits for phase `parity` of `bar`, suspended between probes (so a waiting
+// warp takes no issue slots), giving up after STAGED_WAIT_LIMIT_NS of
+// global time.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  for (uint32_t i = 0; i < (1u << 22); ++i)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    if (mbar_try_wait(bar, parity, 1000000u)) return true;
+    if (global_ns() - t0 > STAGED_WAIT_LIMIT_NS) return false;
+  }
 }
 
 // Bulk copy global -> shared, completion counted on `bar`; the source gets
@@ -326,15 +353,18 @@ __device__ __forceinline__ void staged_loop_init(StagedLoop<CFG>& L) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Waits for phase `parity` of `bar` unless `stop` is raised first.
-// Returns 0 (phase complete), 1 (stopped) or 2 (gave up: bounded).
+// Waits for phase `parity` of `bar` unless `stop` is raised first (looked at
+// every 20 us at most).  Returns 0 (phase complete), 1 (stopped) or 2 (gave
+// up after STAGED_WAIT_LIMIT_NS).
 __device__ __forceinline__ int mbar_wait_or_stop(uint64_t* bar, uint32_t parity,
                                                  const volatile int* stop) {
-  for (uint32_t i = 0; i < (1u << 22); ++i) {
-    if (mbar_try_wait(bar, parity)) return 0;
+  if (mbar_try_wait(bar, parity)) return 0;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    if (mbar_try_wait(bar, parity, 20000u)) return 0;
     if (*stop) return 1;
+    if (global_ns() - t0 > STAGED_WAIT_LIMIT_NS) return 2;
   }
-  return 2;
 }
 
 // Producer: one lane.  On stop (or a wait that gave up, which also sets

@@ -1,10 +1,13 @@
 """Runs the kernels of one workload a few times, for profilers (ncu).
 
     python -m spmv_b200.profile_case --case c2 --reps 3 [--what matvec|cg]
+        [--kernel staged --width 7] [--cg-form 0|2:smem|...]
 
 `matvec` runs the reference matvec demo's loop body (matvecmain.cpp:70-86):
 L2GMap::update then Matrix::mult over all ranks, `reps` times, as plain
-kernel launches.  `cg` runs one spmv::cg solve (a CUDA graph).
+kernel launches.  `cg` runs one spmv::cg solve: a CUDA graph, or one
+cooperative launch of the fused kernel (`--cg-form` forces the form through
+SPMV_B200_CG_FUSED, so no timing launches precede the solve).
 """
 from __future__ import annotations
 
@@ -21,7 +24,12 @@ def main():
     ap.add_argument("--what", default="matvec", choices=["matvec", "cg"])
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--kernel", default="auto", choices=["auto", "vector", "merge", "sell", "staged"])
+    ap.add_argument("--width", type=int, default=0)
+    ap.add_argument("--cg-form", default=None)
     args = ap.parse_args()
+    if args.cg_form is not None:
+        import os
+        os.environ["SPMV_B200_CG_FUSED"] = args.cg_form
 
     import torch
     import spmv_b200 as S
@@ -35,7 +43,7 @@ def main():
     cm = S.L2GMap(comm, D.local_sizes, D.ghosts)
     rm = S.L2GMap(comm, D.local_sizes, [[] for _ in range(W.P)])
     M = S.Matrix(comm, [(rp, ci, va.astype(dt)) for rp, ci, va in D.blocks], cm, rm)
-    M.set_kernel(args.kernel)
+    M.set_kernel(args.kernel, args.width)
     if args.what == "matvec":
         xs = [torch.rand(cm.vec_len(q), dtype=tdt, device="cuda") for q in range(W.P)]
         ys = [torch.empty(D.local_sizes[q], dtype=tdt, device="cuda") for q in range(W.P)]
@@ -48,7 +56,8 @@ def main():
         b = [torch.from_numpy(W.b[D.ranges[q]:D.ranges[q + 1]].copy()).cuda()
              for q in range(W.P)]
         x, k = S.cg(comm, M, b, 10000, W.rtol)
-        print("cg", args.case, "iterations", k)
+        print("cg", args.case, "iterations", k, "form", M.cg_form(), "product",
+              M.solver_product("cg"))
 
 
 if __name__ == "__main__":
