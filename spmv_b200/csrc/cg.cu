@@ -284,42 +284,51 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
   extern __shared__ __align__(128) unsigned char staged_smem[];
   __shared__ StagedLoop<CFG> pipe;
   __shared__ GridSum<NT> gs;
-  // Solver scalars, written by thread 0 between barriers (kept out of the
-  // registers the product phase needs).
+  // The CTA's tiles and rows, and the solver scalars (written by thread 0
+  // between barriers): kept in shared memory, out of the registers the
+  // product phase needs.
+  __shared__ FusedCta me;
   __shared__ struct {
     double rnorm0, rnorm_old, rnorm_new, alpha, beta, pdoty, rtol2;
     int kmax, k, status, go;
   } sv;
 
-  const FusedCta me = ctas[blockIdx.x];
-  const int count = me.t1 - me.t0;
   const int tid = int(threadIdx.x);
-  if (tid == 0) staged_loop_init(pipe);
+  if (tid == 0) {
+    me = ctas[blockIdx.x];
+    staged_loop_init(pipe);
+  }
   __syncthreads();
-  int* err = &c.st->stage_err;
   if (tid >= NT) {
     if (tid == NT)
-      staged_loop_produce<CFG, double, CI>(a, c.tiles + me.t0, count, pipe, staged_smem, err);
+      staged_loop_produce<CFG, double, CI>(a, c.tiles + me.t0, me.t1 - me.t0, pipe,
+                                           staged_smem, &c.st->stage_err);
     return;
   }
-
-  double* rs = reinterpret_cast<double*>(staged_smem + STAGES_BYTES);
-  auto r_at = [&](int g) -> double& { return RS ? rs[g - me.g0] : c.r[g]; };
-  const uint64_t keep = l2_policy_keep();
-  const unsigned long long G = gridDim.x;
+  // r of global row g (this CTA's rows only when RS).
+  auto r_at = [&](int g) -> double& {
+    return RS ? reinterpret_cast<double*>(staged_smem + STAGES_BYTES)[g - me.g0] : c.r[g];
+  };
+  auto grid_sum = [&](double v, double* parts, unsigned long long epoch, double* total) {
+    return coop_grid_sum<NT>(v, parts, c.bar, epoch * gridDim.x, &c.st->stage_err, gs, total);
+  };
 
   // Init: r = p = b, x = 0, rnorm0 = b.b.  Barrier epochs: 1 for the init,
   // 3j+2, 3j+3, 3j+4 for phases A, B, C of iteration j.
   double acc = 0.0;
-  for (int g = me.g0 + tid; g < me.g1; g += NT) {
-    const double bi = c.b[g];
-    r_at(g) = bi;
-    st_pol(c.p + g, bi, keep);
-    st_pol(c.x + g, 0.0, keep);
-    acc += bi * bi;
+  {
+    const uint64_t keep = l2_policy_keep();
+    const int g1 = me.g1;
+    for (int g = me.g0 + tid; g < g1; g += NT) {
+      const double bi = c.b[g];
+      r_at(g) = bi;
+      st_pol(c.p + g, bi, keep);
+      st_pol(c.x + g, 0.0, keep);
+      acc += bi * bi;
+    }
   }
   double rnorm0 = 0.0;
-  bool ok = coop_grid_sum<NT>(acc, c.partials2, c.bar, G, err, gs, &rnorm0);
+  bool ok = grid_sum(acc, c.partials2, 1, &rnorm0);
   if (tid == 0) {
     sv.rtol2 = *static_cast<volatile double*>(&c.st->rtol2);
     sv.kmax = *static_cast<volatile int*>(&c.st->kmax);
@@ -330,32 +339,37 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
     sv.go = ok && sv.kmax > 0 && rnorm0 > 0.0 && isfinite(rnorm0);
   }
   named_sync(1, NT);
+  // Rows per thread in flight in the vector phases: as many as the shape's
+  // registers hold without spilling.
+  constexpr int V = CFG::MINB == 2 ? 4 : CFG::MINB == 3 ? 1 : 2;
   int k = 0;
   while (sv.go) {
-    const unsigned long long e = 3ull * unsigned(k);
     // A: y = A p, p.y.
-    acc = cg_fused_product<CFG, U, CI>(a, count, uint64_t(k) * uint64_t(count), pipe,
-                                       staged_smem, err, c.y, c.p);
+    {
+      const int count = me.t1 - me.t0;
+      acc = cg_fused_product<CFG, U, CI>(a, count, uint64_t(k) * uint64_t(count), pipe,
+                                         staged_smem, &c.st->stage_err, c.y, c.p);
+    }
     double pdoty = 0.0;
-    if (!coop_grid_sum<NT>(acc, c.partials, c.bar, (e + 2) * G, err, gs, &pdoty)) {
+    if (!grid_sum(acc, c.partials, 3ull * unsigned(k) + 2, &pdoty)) {
       ok = false;
       break;
     }
     const bool broke = pdoty == 0.0 || !isfinite(pdoty);
-    const double alpha = sv.rnorm_old / pdoty;
 
-    // B: r -= alpha y, x += alpha p, r.r (skipped after a breakdown); V rows
-    // per thread in flight (r is read when used), as many as the shape's
-    // registers hold without spilling.
-    constexpr int V = CFG::MINB > 1 ? 4 : 2;
+    // B: r -= alpha y, x += alpha p, r.r (skipped after a breakdown; r is
+    // read when used).
     acc = 0.0;
     if (!broke) {
-      for (int g0 = me.g0 + tid; g0 < me.g1; g0 += V * NT) {
+      const double alpha = sv.rnorm_old / pdoty;
+      const uint64_t keep = l2_policy_keep();
+      const int g1 = me.g1;
+      for (int g0 = me.g0 + tid; g0 < g1; g0 += V * NT) {
         double yv[V], pv[V], xv[V];
 #pragma unroll
         for (int u = 0; u < V; ++u) {
           const int g = g0 + u * NT;
-          if (g < me.g1) {
+          if (g < g1) {
             yv[u] = ld_pol(c.y + g, keep);
             pv[u] = ld_pol(c.p + g, keep);
             xv[u] = ld_pol(c.x + g, keep);
@@ -364,7 +378,7 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
 #pragma unroll
         for (int u = 0; u < V; ++u) {
           const int g = g0 + u * NT;
-          if (g < me.g1) {
+          if (g < g1) {
             const double ri = r_at(g) - alpha * yv[u];
             r_at(g) = ri;
             st_pol(c.x + g, xv[u] + alpha * pv[u], keep);
@@ -374,16 +388,16 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
       }
     }
     double rr = 0.0;
-    if (!coop_grid_sum<NT>(acc, c.partials2, c.bar, (e + 3) * G, err, gs, &rr)) {
+    if (!grid_sum(acc, c.partials2, 3ull * unsigned(k) + 3, &rr)) {
       ok = false;
       break;
     }
-    // beta, the count and the convergence test (one thread; every CTA
-    // computes the same from the same totals).
+    // alpha, beta, the count and the convergence test (one thread; every
+    // CTA computes the same from the same totals).
     if (tid == 0) {
       sv.k = k + 1;
       sv.pdoty = pdoty;
-      sv.alpha = alpha;
+      sv.alpha = sv.rnorm_old / pdoty;
       if (broke) {
         sv.status = SPMV_ERROR_BREAKDOWN;
         sv.go = false;
@@ -400,21 +414,26 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
     if (!sv.go) break;
 
     // C: p = p beta + r.
-    const double beta = sv.beta;
-    for (int g0 = me.g0 + tid; g0 < me.g1; g0 += V * NT) {
-      double pv[V];
+    {
+      const double beta = sv.beta;
+      const uint64_t keep = l2_policy_keep();
+      const int g1 = me.g1;
+      for (int g0 = me.g0 + tid; g0 < g1; g0 += V * NT) {
+        double pv[V];
 #pragma unroll
-      for (int u = 0; u < V; ++u) {
-        const int g = g0 + u * NT;
-        if (g < me.g1) pv[u] = ld_pol(c.p + g, keep);
-      }
+        for (int u = 0; u < V; ++u) {
+          const int g = g0 + u * NT;
+          if (g < g1) pv[u] = ld_pol(c.p + g, keep);
+        }
 #pragma unroll
-      for (int u = 0; u < V; ++u) {
-        const int g = g0 + u * NT;
-        if (g < me.g1) st_pol(c.p + g, pv[u] * beta + r_at(g), keep);
+        for (int u = 0; u < V; ++u) {
+          const int g = g0 + u * NT;
+          if (g < g1) st_pol(c.p + g, pv[u] * beta + r_at(g), keep);
+        }
       }
     }
-    if (!coop_grid_barrier<NT>(c.bar, (e + 4) * G, err, gs)) {
+    if (!coop_grid_barrier<NT>(c.bar, (3ull * unsigned(k) + 1) * gridDim.x, &c.st->stage_err,
+                               gs)) {
       ok = false;
       break;
     }
@@ -439,11 +458,12 @@ using FusedFn = void (*)(SpmvArgs, CgPtrs, const FusedCta*);
 
 // Fused shapes: one CTA per SM (28 consumer warps, 6 stages) or two
 // (12 consumer warps, 3 stages each), the rest of shared memory holding r;
-// with r in global memory, two CTAs of 6 stages (the stage bytes per SM of
-// the graph form's product).
+// with r in global memory, two CTAs of 6 stages, or three of 4 (the graph
+// form's product shape, 48 registers per thread).
 using CgFusedOne = StagedCfg<28, 6, 16384>;
 using CgFusedTwo = StagedCfg<12, 3, 16384, 2>;
 using CgFusedTwoDeep = StagedCfg<12, 6, 16384, 2>;
+using CgFusedThree = StagedCfg<12, 4, 16384, 3>;
 
 template <class CFG, bool D16, bool RS>
 FusedFn fused_fn_u(int U) {
@@ -716,6 +736,12 @@ void use_plan(CgWorkspace& w, FusedPlan& plan) {
   w.fused_smem = plan.smem;
   w.fused_cps = plan.cps;
   w.fused_rs = plan.rs;
+  // One partial per CTA in each reduction's array.  partials is baked into
+  // the graph form's kernels and never reallocated: it was sized for more
+  // CTAs than any plan has.
+  require(w.partials.bytes >= sizeof(double) * size_t(plan.grid),
+          "spmv: fused CG grid larger than its partials array");
+  w.partials2.reserve(sizeof(double) * size_t(plan.grid));
   w.ctas.reserve(sizeof(FusedCta) * plan.ctas.size());
   SPMVB_CUDA(cudaMemcpy(w.ctas.ptr, plan.ctas.data(), sizeof(FusedCta) * plan.ctas.size(),
                         cudaMemcpyHostToDevice));
@@ -728,6 +754,10 @@ void enqueue_solve(CgWorkspace& w, cudaStream_t s) {
                 "rtol2 .. stage_err are one contiguous block");
   SPMVB_CUDA(cudaMemcpyAsync(&st->rtol2, &w.host.rtol2, 32, cudaMemcpyHostToDevice, s));
   if (w.fused) {
+    const size_t g = size_t(w.fused_grid);
+    require(w.partials.bytes >= g * sizeof(double) && w.partials2.bytes >= g * sizeof(double) &&
+                w.ctas.bytes >= g * sizeof(FusedCta),
+            "spmv: fused CG buffers smaller than its grid");
     SPMVB_CUDA(cudaMemsetAsync(w.bar.ptr, 0, sizeof(unsigned long long), s));
     CgPtrs c = cg_ptrs(w);
     const FusedCta* ctas = w.ctas.as<FusedCta>();
@@ -776,8 +806,8 @@ float time_iterations(CgWorkspace& w, cudaStream_t s, int its) {
 // few iterations of each on b = 1: r in shared memory with one or two CTAs
 // per SM (when the CTAs' rows fit), and two CTAs per SM of deeper pipelines
 // with r in global memory.  SPMV_B200_CG_FUSED: "0" keeps the graph form;
-// "<cps>:<smem|global>" forces that plan (1:global is the one-CTA shape),
-// failing if it does not fit.
+// "<cps>:<smem|global>" forces that plan (1:smem, 2:smem, 1:global,
+// 2:global, 3:global), failing if it does not fit.
 void choose_form(spmv_matrix A, CgWorkspace& w) {
   w.fused = false;
   if (w.product.kind != ProductKind::Staged || w.n == 0) return;
@@ -789,7 +819,6 @@ void choose_form(spmv_matrix A, CgWorkspace& w) {
   SPMVB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, comm->device));
   if (!coop) return;
   w.bar.reserve(sizeof(unsigned long long));
-  w.partials2.reserve(sizeof(double) * std::max(1, comm->num_sms) * 2);
   w.fused_args = k1_args(A, w, w.product);
 
   const SolverProduct& sp = w.product;
@@ -800,8 +829,9 @@ void choose_form(spmv_matrix A, CgWorkspace& w) {
     else if (mode == "2:smem") fits = plan_fused<CgFusedTwo, true>(A, sp, p);
     else if (mode == "1:global") fits = plan_fused<CgFusedOne, false>(A, sp, p);
     else if (mode == "2:global") fits = plan_fused<CgFusedTwoDeep, false>(A, sp, p);
+    else if (mode == "3:global") fits = plan_fused<CgFusedThree, false>(A, sp, p);
     require(fits, "spmv: SPMV_B200_CG_FUSED must be 0 or a fused plan that fits this matrix "
-                  "(1:smem, 2:smem, 1:global, 2:global)");
+                  "(1:smem, 2:smem, 1:global, 2:global, 3:global)");
     use_plan(w, p);
     return;
   }
@@ -811,6 +841,8 @@ void choose_form(spmv_matrix A, CgWorkspace& w) {
     if (plan_fused<CgFusedOne, true>(A, sp, p1)) plans.push_back(std::move(p1));
     if (plan_fused<CgFusedTwo, true>(A, sp, p2)) plans.push_back(std::move(p2));
     if (plan_fused<CgFusedTwoDeep, false>(A, sp, p3)) plans.push_back(std::move(p3));
+    FusedPlan p4;
+    if (plan_fused<CgFusedThree, false>(A, sp, p4)) plans.push_back(std::move(p4));
   }
   if (plans.empty()) return;
   cudaStream_t s = A->comm->stream;

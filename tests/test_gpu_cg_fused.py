@@ -13,7 +13,7 @@ from helpers import build
 
 pytestmark = pytest.mark.gpu
 
-PLANS = ["1:smem", "2:smem", "1:global", "2:global"]
+PLANS = ["1:smem", "2:smem", "1:global", "2:global", "3:global"]
 
 
 def setup(monkeypatch, plan, W, P, width=8):
