@@ -247,8 +247,9 @@ int spmv_matrix_mult_noalloc(spmv_matrix A, const void* const* x,
                              void* const* y);
 /* Kernel choice.  width: lanes per row for SPMV_KERNEL_VECTOR (1..32, a
  * power of two), loads in flight per lane for SPMV_KERNEL_SELL (1..16, a
- * power of two), gathers in flight per lane for SPMV_KERNEL_STAGED (4, 5, 7
- * or 8; 5 and 7 suit stencils whose rows have exactly that many entries);
+ * power of two), gathers in flight per lane for SPMV_KERNEL_STAGED (4, 5, 7,
+ * 8 or 9; 5, 7 and 9 suit stencils whose rows have a multiple of that many
+ * entries: 5-, 7- and 27-point);
  * 0 = from statistics; block: threads per CTA (0 = default). */
 int spmv_matrix_set_kernel(spmv_matrix A, spmv_kernel kernel, int width,
                            int block);

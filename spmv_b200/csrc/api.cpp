@@ -898,8 +898,8 @@ int spmv_matrix_set_kernel(spmv_matrix A, spmv_kernel kernel, int width,
     require(kernel != SPMV_KERNEL_SELL || width <= 16,
             "spmv: SELL width (loads in flight per lane) must be 1..16");
     require(kernel != SPMV_KERNEL_STAGED || width == 0 || width == 4 || width == 5 ||
-                width == 7 || width == 8,
-            "spmv: staged width (gathers in flight per lane) must be 4, 5, 7 or 8");
+                width == 7 || width == 8 || width == 9,
+            "spmv: staged width (gathers in flight per lane) must be 4, 5, 7, 8 or 9");
     require(block == 0 || block == 128 || block == 256 || block == 512,
             "spmv: block must be 0, 128, 256 or 512");
     A->kernel = kernel;

@@ -469,6 +469,7 @@ template <class CFG, bool D16, bool RS>
 FusedFn fused_fn_u(int U) {
   switch (staged_width(U)) {
     case 8: return cg_fused<CFG, 8, D16, RS>;
+    case 9: return cg_fused<CFG, 9, D16, RS>;
     case 7: return cg_fused<CFG, 7, D16, RS>;
     case 5: return cg_fused<CFG, 5, D16, RS>;
     default: return cg_fused<CFG, 4, D16, RS>;
@@ -511,6 +512,7 @@ template <bool D16, bool H>
 K1Fn k1_staged(int U) {
   switch (staged_width(U)) {
     case 8: return cg_k1_staged<8, D16, H>;
+    case 9: return cg_k1_staged<9, D16, H>;
     case 7: return cg_k1_staged<7, D16, H>;
     case 5: return cg_k1_staged<5, D16, H>;
     default: return cg_k1_staged<4, D16, H>;

@@ -346,7 +346,16 @@ enum class ProductKind : int {
 };
 // Gathers in flight per lane of the staged product: 4, 8, or a stencil's
 // exact row width 5 or 7 (one unmasked chunk per slice).
-inline int staged_width(int w) { return w >= 8 ? 8 : (w == 7 || w == 5) ? w : 4; }
+inline int staged_width(int w) {
+  return w == 9 ? 9 : w >= 8 ? 8 : (w == 7 || w == 5) ? w : 4;
+}
+// The staged width that divides a stencil's longest row exactly (9, 7 or 5,
+// so its full slices take the unmasked path), or 0.
+inline int exact_staged_width(int64_t max_row) {
+  for (int u : {9, 7, 5})
+    if (max_row > 0 && max_row % u == 0 && max_row <= 4 * u) return u;
+  return 0;
+}
 struct SolverProduct {
   ProductKind kind = ProductKind::Vector;
   int w = 0;

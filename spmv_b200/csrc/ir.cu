@@ -328,6 +328,7 @@ K1 pick_k1(int W) {
   if constexpr (KIND == 2) {
     switch (staged_width(W)) {
       case 8: return ir_spmv_dot_staged<8, D16, H>;
+      case 9: return ir_spmv_dot_staged<9, D16, H>;
       case 7: return ir_spmv_dot_staged<7, D16, H>;
       case 5: return ir_spmv_dot_staged<5, D16, H>;
       default: return ir_spmv_dot_staged<4, D16, H>;
@@ -349,6 +350,7 @@ KR pick_kr(int W) {
   if constexpr (KIND == 2) {
     switch (staged_width(W)) {
       case 8: return ir_residual_staged<8, D16>;
+      case 9: return ir_residual_staged<9, D16>;
       case 7: return ir_residual_staged<7, D16>;
       case 5: return ir_residual_staged<5, D16>;
       default: return ir_residual_staged<4, D16>;

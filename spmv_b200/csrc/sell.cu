@@ -372,7 +372,8 @@ template <typename T>
 void launch_staged_t(const SpmvLaunch& L, const SpmvArgs& a, const DevCsr::StagedTable& t,
                      int U, cudaStream_t s) {
   const int u = staged_width(U);
-  const void* fn = u == 8   ? (const void*)spmv_staged_kernel<T, int32_t, 8>
+  const void* fn = u == 9   ? (const void*)spmv_staged_kernel<T, int32_t, 9>
+                   : u == 8 ? (const void*)spmv_staged_kernel<T, int32_t, 8>
                    : u == 7 ? (const void*)spmv_staged_kernel<T, int32_t, 7>
                    : u == 5 ? (const void*)spmv_staged_kernel<T, int32_t, 5>
                             : (const void*)spmv_staged_kernel<T, int32_t, 4>;

@@ -163,6 +163,10 @@ __device__ __forceinline__ void staged_tile_rows(const SpmvArgs& a,
                                                  int lane, int& q0, F&& f, const G& gx) {
   constexpr int NC = CFG::NC;
   constexpr int MAXE = CFG::max_entries(int(sizeof(T) + sizeof(CI)));
+  // Multi-chunk unmasked slices only where a stencil's rows are several
+  // chunks long (U = 9 for 27 entries); the other widths keep their
+  // measured code.
+  constexpr bool UNMASKED_CHUNKS = U == 9;
   const StagedDesc* h = reinterpret_cast<const StagedDesc*>(stage);
   const T* sv = reinterpret_cast<const T*>(stage + STAGED_HEADER_BYTES);
   const CI* sc = reinterpret_cast<const CI*>(stage + STAGED_HEADER_BYTES + MAXE * int(sizeof(T)));
@@ -176,7 +180,7 @@ __device__ __forceinline__ void staged_tile_rows(const SpmvArgs& a,
     const int row = (h->s0 + j) * 32 + lane;
     const int g = P.row0 + row;
     T sum = T(0);
-    if (w == U) {
+    if (!UNMASKED_CHUNKS && w == U) {
       // The slice's rows in one chunk: no slot masks.  A padding entry
       // gathers x[0] (in bounds in every layout; the value is not used).
       T v[U], xv[U];
@@ -195,6 +199,25 @@ __device__ __forceinline__ void staged_tile_rows(const SpmvArgs& a,
 #pragma unroll
       for (int u = 0; u < U; ++u)
         if (ok[u]) sum += v[u] * xv[u];
+      if (row < P.nrows) f(P, row, sum);
+      continue;
+    }
+    if (UNMASKED_CHUNKS && w % U == 0) {
+      // Whole chunks (27 entries at U = 9): the same, chunk by chunk, values
+      // read from shared memory when summed (fewer registers held).
+      for (int k0 = 0; k0 < w; k0 += U) {
+        T xv[U];
+        bool ok[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int ci = int(sc[o + (k0 + u) * 32 + lane]);
+          ok[u] = sizeof(CI) == 2 ? ci != -32768 : ci >= 0;
+          xv[u] = gx(P, ok[u] ? (sizeof(CI) == 2 ? g + ci : ci) : 0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (ok[u]) sum += sv[o + (k0 + u) * 32 + lane] * xv[u];
+      }
       if (row < P.nrows) f(P, row, sum);
       continue;
     }

@@ -167,9 +167,10 @@ SolverProduct choose_solver_product(spmv_matrix A, spmv_dtype dt, const void* x,
           cands.push_back({ProductKind::Staged, staged_width(A->width), d, 0.f});
         } else {
           for (int u : {4, 8}) cands.push_back({ProductKind::Staged, u, d, 0.f});
-          // A stencil whose rows all have 5 or 7 entries: one unmasked chunk.
-          if (C.max_row == 5 || C.max_row == 7)
-            cands.push_back({ProductKind::Staged, int(C.max_row), d, 0.f});
+          // A stencil whose longest row is a multiple of 9, 7 or 5 entries:
+          // its full slices take the unmasked path.
+          if (exact_staged_width(C.max_row) > 0)
+            cands.push_back({ProductKind::Staged, exact_staged_width(C.max_row), d, 0.f});
         }
       }
     }

@@ -126,8 +126,8 @@ void autotune(spmv_matrix A, int reps, spmv_tune_result* best) {
     for (const DevPart& D : C.parts) nnz += D.nnz;
     if (C.sell_padded <= 2 * std::max<int64_t>(nnz, 1))
       for (int u : {4, 8}) cands.push_back({SPMV_KERNEL_STAGED, u, 0});
-    if (C.sell_padded <= 2 * std::max<int64_t>(nnz, 1) && (C.max_row == 5 || C.max_row == 7))
-      cands.push_back({SPMV_KERNEL_STAGED, int(C.max_row), 0});
+    if (C.sell_padded <= 2 * std::max<int64_t>(nnz, 1) && exact_staged_width(C.max_row) > 0)
+      cands.push_back({SPMV_KERNEL_STAGED, exact_staged_width(C.max_row), 0});
     cands.push_back({SPMV_KERNEL_MERGE, 0, 256});
   }
 

@@ -37,7 +37,8 @@ def true_relres(W, x):
 
 @pytest.mark.parametrize("plan", PLANS)
 @pytest.mark.parametrize("cfg,scale,P,width", [("c2", 32, 8, 8), ("c2", 40, 3, 4),
-                                               ("c2", 32, 8, 7), ("c1", 64, 3, 5)])
+                                               ("c2", 32, 8, 7), ("c1", 64, 3, 5),
+                                               ("c3", 24, 2, 9)])
 def test_fused_matches_graph_form(monkeypatch, cuda_device, plan, cfg, scale, P, width):
     """Same per-element arithmetic as the graph form; only the grouping of
     the two dot products' partial sums differs."""
@@ -97,11 +98,11 @@ def test_fused_plan_that_does_not_fit_is_refused(monkeypatch, cuda_device):
 
 
 def test_staged_widths_accepted(cuda_device):
-    """Staged widths are gathers in flight: 4, 5, 7 or 8 (5 and 7 are a
-    stencil's exact row lengths); others are refused."""
+    """Staged widths are gathers in flight: 4, 5, 7, 8 or 9 (5, 7 and 9
+    divide the 5-, 7- and 27-point stencils' rows); others are refused."""
     W = gen.workload("c2", 16)
     comm, cm, rm, M, D = build(W, 2)
-    for w in (4, 5, 7, 8):
+    for w in (4, 5, 7, 8, 9):
         M.set_kernel("staged", w)
         assert M.get_kernel()[:2] == ("staged", w)
     with pytest.raises(S.SpmvError):

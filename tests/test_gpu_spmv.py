@@ -199,10 +199,12 @@ def test_sell_is_bitwise_equal_to_oracle(cuda_device, cfg, P):
                                                        xs[q].astype(np.float32)))
 
 
-@pytest.mark.parametrize("cfg,P,width", [("c1", 1, 8), ("c2", 8, 4), ("c2", 3, 8), ("c3", 1, 8)])
+@pytest.mark.parametrize("cfg,P,width", [("c1", 1, 8), ("c2", 8, 4), ("c2", 3, 8), ("c3", 1, 8),
+                                         ("c1", 2, 5), ("c2", 8, 7), ("c3", 1, 9), ("c3", 3, 9)])
 def test_staged_is_bitwise_equal_to_oracle(cuda_device, cfg, P, width):
     # The staged SELL-32 product (tiles streamed into shared memory by bulk
-    # copies) also sums rows in storage order.
+    # copies) also sums rows in storage order; widths 5, 7 and 9 take the
+    # unmasked path on the 5-, 7- and 27-point stencils' full slices.
     W = gen.workload(cfg, scale=0 if cfg != "c3" else 40)
     comm, cm, rm, M, D = build(W, P)
     M.set_kernel("staged", width)
