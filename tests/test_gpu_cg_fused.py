@@ -109,3 +109,27 @@ def test_staged_widths_accepted(cuda_device):
         M.set_kernel("staged", 6)
     with pytest.raises(S.SpmvError):
         M.set_kernel("sell", 7)
+
+
+@pytest.mark.parametrize("plan", ["2:smem", "3:global"])
+def test_fused_with_an_empty_rank_and_unaligned_ranks(monkeypatch, cuda_device, plan):
+    """Ranks of 300, 0 and 724 rows (the last rank's rows start off the
+    32-row slice grid; the middle rank owns nothing): the fused solve gives
+    the graph form's answer."""
+    W = gen.workload("c1", 32)
+    monkeypatch.setattr(gen, "owner_ranges", lambda P, n: np.array([0, 300, 300, n]))
+    out = {}
+    for mode in ("0", plan):
+        monkeypatch.setenv("SPMV_B200_CG_FUSED", mode)
+        comm, cm, rm, M, D = build(W, 3)
+        assert D.local_sizes == [300, 0, W.A.nrows - 300]
+        M.set_kernel("staged", 5)
+        b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(3)]
+        x, k, info = S.cg(comm, M, b, 10000, W.rtol, info=True)
+        assert info.status == 0 and M.cg_form()[0] == ("graph" if mode == "0" else "fused")
+        assert x[1].size == 0
+        out[mode] = (np.concatenate([x[q][:D.local_sizes[q]] for q in range(3)]), k)
+    (x0, k0), (x1, k1) = out["0"], out[plan]
+    assert abs(k1 - k0) <= 2
+    assert np.linalg.norm(x1 - x0) <= 1e-9 * np.linalg.norm(x0)
+    assert true_relres(W, x1) < 1.5 * W.rtol
