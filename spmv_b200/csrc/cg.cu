@@ -240,9 +240,10 @@ __global__ void __launch_bounds__(EW_BS) cg_update_xp(const CgPtrs c) {
 //   A  y = A p over the CTA's tiles (the staged traversal; its producer warp
 //      keeps streaming the same tiles pass after pass, so the next pass's
 //      first tiles land during B and C), p.y          -> barrier, alpha
-//   B  r -= alpha y, x += alpha p on the CTA's rows, r.r -> barrier, beta,
+//   B  r -= alpha y on the CTA's rows, r.r           -> barrier, beta,
 //      count, convergence test (identical in every CTA)
-//   C  p = p beta + r on the CTA's rows               -> barrier (A gathers p)
+//   C  x += alpha p, p = p beta + r on the CTA's rows -> barrier (A gathers p)
+//      (in the last iteration x only)
 //
 // RS: r lives in shared memory for the whole solve (only this CTA's rows
 // ever read it), so it never crosses HBM.  The arithmetic of every vector
@@ -357,23 +358,18 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
     }
     const bool broke = pdoty == 0.0 || !isfinite(pdoty);
 
-    // B: r -= alpha y, x += alpha p, r.r (skipped after a breakdown; r is
-    // read when used).
+    // B: r -= alpha y, r.r (skipped after a breakdown; r is read when used).
     acc = 0.0;
     if (!broke) {
       const double alpha = sv.rnorm_old / pdoty;
       const uint64_t keep = l2_policy_keep();
       const int g1 = me.g1;
       for (int g0 = me.g0 + tid; g0 < g1; g0 += V * NT) {
-        double yv[V], pv[V], xv[V];
+        double yv[V];
 #pragma unroll
         for (int u = 0; u < V; ++u) {
           const int g = g0 + u * NT;
-          if (g < g1) {
-            yv[u] = ld_pol(c.y + g, keep);
-            pv[u] = ld_pol(c.p + g, keep);
-            xv[u] = ld_pol(c.x + g, keep);
-          }
+          if (g < g1) yv[u] = ld_pol(c.y + g, keep);
         }
 #pragma unroll
         for (int u = 0; u < V; ++u) {
@@ -381,7 +377,6 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
           if (g < g1) {
             const double ri = r_at(g) - alpha * yv[u];
             r_at(g) = ri;
-            st_pol(c.x + g, xv[u] + alpha * pv[u], keep);
             acc += ri * ri;
           }
         }
@@ -411,26 +406,35 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
     }
     named_sync(1, NT);
     k += 1;
-    if (!sv.go) break;
+    if (broke) break;
 
-    // C: p = p beta + r.
+    // C: x += alpha p (this iteration's alpha and p), then, unless the solve
+    // stops here, p = p beta + r.
     {
-      const double beta = sv.beta;
+      const double alpha = sv.alpha, beta = sv.beta;
+      const bool go = sv.go;
       const uint64_t keep = l2_policy_keep();
       const int g1 = me.g1;
       for (int g0 = me.g0 + tid; g0 < g1; g0 += V * NT) {
-        double pv[V];
+        double pv[V], xv[V];
 #pragma unroll
         for (int u = 0; u < V; ++u) {
           const int g = g0 + u * NT;
-          if (g < g1) pv[u] = ld_pol(c.p + g, keep);
+          if (g < g1) {
+            pv[u] = ld_pol(c.p + g, keep);
+            xv[u] = ld_pol(c.x + g, keep);
+          }
         }
 #pragma unroll
         for (int u = 0; u < V; ++u) {
           const int g = g0 + u * NT;
-          if (g < g1) st_pol(c.p + g, pv[u] * beta + r_at(g), keep);
+          if (g < g1) {
+            st_pol(c.x + g, xv[u] + alpha * pv[u], keep);
+            if (go) st_pol(c.p + g, pv[u] * beta + r_at(g), keep);
+          }
         }
       }
+      if (!go) break;
     }
     if (!coop_grid_barrier<NT>(c.bar, (3ull * unsigned(k) + 1) * gridDim.x, &c.st->stage_err,
                                gs)) {
