@@ -768,11 +768,19 @@ void enqueue_solve(CgWorkspace& w, cudaStream_t s) {
     CgPtrs c = cg_ptrs(w);
     const FusedCta* ctas = w.ctas.as<FusedCta>();
     void* args[] = {&w.fused_args, &c, &ctas};
-    SPMVB_CUDA(cudaLaunchCooperativeKernel(w.fused_fn, dim3(w.fused_grid), dim3(w.fused_block),
-                                           args, size_t(w.fused_smem), s));
-  } else {
-    SPMVB_CUDA(cudaGraphLaunch(w.exec, s));
+    const cudaError_t e = cudaLaunchCooperativeKernel(
+        w.fused_fn, dim3(w.fused_grid), dim3(w.fused_block), args, size_t(w.fused_smem), s);
+    if (e != cudaErrorCooperativeLaunchTooLarge) {
+      SPMVB_CUDA(e);
+      return;
+    }
+    // The grid no longer fits on the device at once (a context given fewer
+    // SMs than the plan was made for): this solve and the later ones run in
+    // the graph form.  The error is a refused launch; nothing ran.
+    (void)cudaGetLastError();
+    w.fused = false;
   }
+  SPMVB_CUDA(cudaGraphLaunch(w.exec, s));
 }
 
 __global__ void cg_fill(double* v, int64_t n, double value) {
@@ -861,6 +869,7 @@ void choose_form(spmv_matrix A, CgWorkspace& w) {
   for (size_t i = 0; i < plans.size(); ++i) {
     use_plan(w, plans[i]);
     const float t = time_iterations(w, s, its);
+    if (!w.fused) continue;  // the plan's launch was refused (graph form ran)
     if (t < best) {
       best = t;
       pick = int(i);
