@@ -275,45 +275,28 @@ __device__ __forceinline__ double cg_fused_product(const SpmvArgs& a, int count,
   return acc;
 }
 
-template <class CFG, int U, bool D16, bool RS>
-__global__ void __launch_bounds__(CFG::BS, CFG::MINB)
-    cg_fused(const __grid_constant__ SpmvArgs a, const CgPtrs c,
-             const FusedCta* __restrict__ ctas) {
-  using CI = typename std::conditional<D16, int16_t, int32_t>::type;
-  constexpr int NT = CFG::NC * 32;
-  constexpr int STAGES_BYTES = CFG::smem_bytes(8 + int(sizeof(CI)));
-  extern __shared__ __align__(128) unsigned char staged_smem[];
-  __shared__ StagedLoop<CFG> pipe;
-  __shared__ GridSum<NT> gs;
-  // The CTA's tiles and rows, and the solver scalars (written by thread 0
-  // between barriers): kept in shared memory, out of the registers the
-  // product phase needs.
-  __shared__ FusedCta me;
-  __shared__ struct {
-    double rnorm0, rnorm_old, rnorm_new, alpha, beta, pdoty, rtol2;
-    int kmax, k, status, go;
-  } sv;
+// Solver scalars of the fused solve (one copy per CTA, in shared memory,
+// written by thread 0 between barriers).
+struct FusedScalars {
+  double rnorm0, rnorm_old, rnorm_new, alpha, beta, pdoty, rtol2;
+  int kmax, k, status, go;
+};
 
+// The fused solve after its CTA's set-up, for the NT consumer threads (the
+// CTA's first NT): init, then per iteration phase A = product(k) (this
+// thread's share of p.y after y = A p over the CTA's rows), B and C with the
+// grid barriers between; V rows per thread in flight in the vector phases;
+// r_at(g): r of the CTA's global row g.  Thread 0 of CTA 0 writes the final
+// state.  Returns false when a bounded wait failed (the error flag is
+// raised).
+template <int NT, int V, class RAt, class Product>
+__device__ __forceinline__ bool cg_fused_solve(const CgPtrs& c, const FusedCta& me,
+                                               GridSum<NT>& gs, FusedScalars& sv, RAt&& r_at,
+                                               Product&& product) {
   const int tid = int(threadIdx.x);
-  if (tid == 0) {
-    me = ctas[blockIdx.x];
-    staged_loop_init(pipe);
-  }
-  __syncthreads();
-  if (tid >= NT) {
-    if (tid == NT)
-      staged_loop_produce<CFG, double, CI>(a, c.tiles + me.t0, me.t1 - me.t0, pipe,
-                                           staged_smem, &c.st->stage_err);
-    return;
-  }
-  // r of global row g (this CTA's rows only when RS).
-  auto r_at = [&](int g) -> double& {
-    return RS ? reinterpret_cast<double*>(staged_smem + STAGES_BYTES)[g - me.g0] : c.r[g];
-  };
   auto grid_sum = [&](double v, double* parts, unsigned long long epoch, double* total) {
     return coop_grid_sum<NT>(v, parts, c.bar, epoch * gridDim.x, &c.st->stage_err, gs, total);
   };
-
   // Init: r = p = b, x = 0, rnorm0 = b.b.  Barrier epochs: 1 for the init,
   // 3j+2, 3j+3, 3j+4 for phases A, B, C of iteration j.
   double acc = 0.0;
@@ -340,17 +323,10 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
     sv.go = ok && sv.kmax > 0 && rnorm0 > 0.0 && isfinite(rnorm0);
   }
   named_sync(1, NT);
-  // Rows per thread in flight in the vector phases: as many as the shape's
-  // registers hold without spilling.
-  constexpr int V = CFG::MINB == 2 ? 4 : CFG::MINB == 3 ? 1 : 2;
   int k = 0;
   while (sv.go) {
     // A: y = A p, p.y.
-    {
-      const int count = me.t1 - me.t0;
-      acc = cg_fused_product<CFG, U, CI>(a, count, uint64_t(k) * uint64_t(count), pipe,
-                                         staged_smem, &c.st->stage_err, c.y, c.p);
-    }
+    acc = product(k);
     double pdoty = 0.0;
     if (!grid_sum(acc, c.partials, 3ull * unsigned(k) + 2, &pdoty)) {
       ok = false;
@@ -442,20 +418,60 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
       break;
     }
   }
-  if (tid == 0) {
-    pipe.stop = 1;
-    if (ok && blockIdx.x == 0) {
-      CgState* st = c.st;
-      st->rnorm0 = sv.rnorm0;
-      st->rnorm_old = sv.rnorm_old;
-      st->rnorm_new = sv.rnorm_new;
-      st->alpha = sv.alpha;
-      st->beta = sv.beta;
-      st->pdoty = sv.pdoty;
-      st->k = sv.k;
-      st->status = sv.status;
-    }
+  if (tid == 0 && ok && blockIdx.x == 0) {
+    CgState* st = c.st;
+    st->rnorm0 = sv.rnorm0;
+    st->rnorm_old = sv.rnorm_old;
+    st->rnorm_new = sv.rnorm_new;
+    st->alpha = sv.alpha;
+    st->beta = sv.beta;
+    st->pdoty = sv.pdoty;
+    st->k = sv.k;
+    st->status = sv.status;
   }
+  return ok;
+}
+
+template <class CFG, int U, bool D16, bool RS>
+__global__ void __launch_bounds__(CFG::BS, CFG::MINB)
+    cg_fused(const __grid_constant__ SpmvArgs a, const CgPtrs c,
+             const FusedCta* __restrict__ ctas) {
+  using CI = typename std::conditional<D16, int16_t, int32_t>::type;
+  constexpr int NT = CFG::NC * 32;
+  constexpr int STAGES_BYTES = CFG::smem_bytes(8 + int(sizeof(CI)));
+  // Rows per thread in flight in the vector phases: as many as the shape's
+  // registers hold without spilling.
+  constexpr int V = CFG::MINB == 2 ? 4 : CFG::MINB == 3 ? 1 : 2;
+  extern __shared__ __align__(128) unsigned char staged_smem[];
+  __shared__ StagedLoop<CFG> pipe;
+  __shared__ GridSum<NT> gs;
+  // The CTA's tiles and rows, and the solver scalars: kept in shared memory,
+  // out of the registers the product phase needs.
+  __shared__ FusedCta me;
+  __shared__ FusedScalars sv;
+
+  const int tid = int(threadIdx.x);
+  if (tid == 0) {
+    me = ctas[blockIdx.x];
+    staged_loop_init(pipe);
+  }
+  __syncthreads();
+  if (tid >= NT) {
+    if (tid == NT)
+      staged_loop_produce<CFG, double, CI>(a, c.tiles + me.t0, me.t1 - me.t0, pipe,
+                                           staged_smem, &c.st->stage_err);
+    return;
+  }
+  // r of global row g (this CTA's rows only when RS).
+  auto r_at = [&](int g) -> double& {
+    return RS ? reinterpret_cast<double*>(staged_smem + STAGES_BYTES)[g - me.g0] : c.r[g];
+  };
+  cg_fused_solve<NT, V>(c, me, gs, sv, r_at, [&](int k) {
+    const int count = me.t1 - me.t0;
+    return cg_fused_product<CFG, U, CI>(a, count, uint64_t(k) * uint64_t(count), pipe,
+                                        staged_smem, &c.st->stage_err, c.y, c.p);
+  });
+  if (tid == 0) pipe.stop = 1;
 }
 
 using FusedFn = void (*)(SpmvArgs, CgPtrs, const FusedCta*);
@@ -484,6 +500,7 @@ template <class CFG, bool RS>
 FusedFn fused_fn(const SolverProduct& sp) {
   return sp.d16 ? fused_fn_u<CFG, true, RS>(sp.w) : fused_fn_u<CFG, false, RS>(sp.w);
 }
+
 
 using K1Fn = void (*)(SpmvArgs, CgPtrs, cudaGraphConditionalHandle);
 
@@ -696,24 +713,19 @@ struct FusedPlan {
   std::vector<FusedCta> ctas;
 };
 
-// A plan for shape CFG (CFG::MINB CTAs per SM), r in shared memory (RS) or
-// global memory; false when it does not fit.
-template <class CFG, bool RS>
-bool plan_fused(spmv_matrix A, const SolverProduct& sp, FusedPlan& plan) {
-  const int cps = CFG::MINB;
-  const bool rs = RS;
-  const int eb = 8 + (sp.d16 ? 2 : 4);
-  static_assert(CFG::max_entries(10) == SolverStaged::max_entries(10) &&
-                    CFG::max_entries(12) == SolverStaged::max_entries(12),
-                "fused shapes use the solver product's tiles");
+// A plan for kernel `fn` of `block` threads at `cps` CTAs per SM, with
+// `stage_smem` bytes of stage buffers and r in shared memory (rs) or global
+// memory; false when it does not fit.
+bool plan_common(spmv_matrix A, const SolverProduct& sp, const void* fn, int block, int cps,
+                 int64_t stage_smem, bool rs, FusedPlan& plan) {
+  if (!fn) return false;
   const DevCsr::StagedTable& t = cg_tiles(A, sp);
   if (!t.ok) return false;
   spmv_comm comm = A->comm;
   const int grid = std::max(1, comm->num_sms) * cps;
   std::vector<FusedCta> ctas;
   const int64_t longest = fused_ctas(A, t, grid, ctas);
-  const int64_t smem = CFG::smem_bytes(eb) + (rs ? (longest * 8 + 15) / 16 * 16 : 0);
-  const void* fn = (const void*)fused_fn<CFG, RS>(sp);
+  const int64_t smem = stage_smem + (rs ? (longest * 8 + 15) / 16 * 16 : 0);
   int optin = 0;
   SPMVB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
                                     comm->device));
@@ -722,16 +734,27 @@ bool plan_fused(spmv_matrix A, const SolverProduct& sp, FusedPlan& plan) {
   if (smem + int64_t(fa.sharedSizeBytes) > optin) return false;
   SPMVB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   int nb = 0;
-  SPMVB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, CFG::BS, size_t(smem)));
+  SPMVB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, size_t(smem)));
   if (nb < cps) return false;
   plan.fn = fn;
   plan.grid = grid;
-  plan.block = CFG::BS;
+  plan.block = block;
   plan.smem = int(smem);
   plan.cps = cps;
   plan.rs = rs;
   plan.ctas = std::move(ctas);
   return true;
+}
+
+// Staged product: shape CFG (CFG::MINB CTAs per SM).
+template <class CFG, bool RS>
+bool plan_fused(spmv_matrix A, const SolverProduct& sp, FusedPlan& plan) {
+  static_assert(CFG::max_entries(10) == SolverStaged::max_entries(10) &&
+                    CFG::max_entries(12) == SolverStaged::max_entries(12),
+                "fused shapes use the solver product's tiles");
+  const int eb = 8 + (sp.d16 ? 2 : 4);
+  return plan_common(A, sp, (const void*)fused_fn<CFG, RS>(sp), CFG::BS, CFG::MINB,
+                     CFG::smem_bytes(eb), RS, plan);
 }
 
 void use_plan(CgWorkspace& w, FusedPlan& plan) {
@@ -762,7 +785,7 @@ void enqueue_solve(CgWorkspace& w, cudaStream_t s) {
   if (w.fused) {
     const size_t g = size_t(w.fused_grid);
     require(w.partials.bytes >= g * sizeof(double) && w.partials2.bytes >= g * sizeof(double) &&
-                w.ctas.bytes >= g * sizeof(FusedCta),
+                w.ctas.bytes >= g * sizeof(FusedCta) && w.tiles != nullptr,
             "spmv: fused CG buffers smaller than its grid");
     SPMVB_CUDA(cudaMemsetAsync(w.bar.ptr, 0, sizeof(unsigned long long), s));
     CgPtrs c = cg_ptrs(w);
@@ -817,14 +840,16 @@ float time_iterations(CgWorkspace& w, cudaStream_t s, int its) {
 }
 
 // Chooses between the graph form and the fused plans that fit, by timing a
-// few iterations of each on b = 1: r in shared memory with one or two CTAs
-// per SM (when the CTAs' rows fit), and two CTAs per SM of deeper pipelines
-// with r in global memory.  SPMV_B200_CG_FUSED: "0" keeps the graph form;
-// "<cps>:<smem|global>" forces that plan (1:smem, 2:smem, 1:global,
-// 2:global, 3:global), failing if it does not fit.
+// few iterations of each on b = 1 (the fused form needs a staged product):
+// r in shared memory with one or two CTAs per SM (when the CTAs' rows fit),
+// or r in global memory with two CTAs of 6 stages or three of 4.
+// SPMV_B200_CG_FUSED: "0" keeps the graph form; "<cps>:<smem|global>"
+// forces that plan (1:smem, 2:smem, 1:global, 2:global, 3:global), failing
+// if it does not fit.
 void choose_form(spmv_matrix A, CgWorkspace& w) {
   w.fused = false;
-  if (w.product.kind != ProductKind::Staged || w.n == 0) return;
+  const SolverProduct& sp = w.product;
+  if (sp.kind != ProductKind::Staged || w.n == 0) return;
   const char* env = std::getenv("SPMV_B200_CG_FUSED");
   const std::string mode = env ? env : "";
   if (mode == "0") return;
@@ -832,10 +857,14 @@ void choose_form(spmv_matrix A, CgWorkspace& w) {
   int coop = 0;
   SPMVB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, comm->device));
   if (!coop) return;
+  // The fused kernel streams the product's tile table.
+  const DevCsr::StagedTable& tiles = cg_tiles(A, sp);
+  if (!tiles.ok) return;
+  w.tiles = tiles.desc.as<StagedDesc>();
+  w.ntiles = tiles.ntiles;
   w.bar.reserve(sizeof(unsigned long long));
   w.fused_args = k1_args(A, w, w.product);
 
-  const SolverProduct& sp = w.product;
   if (!mode.empty()) {
     FusedPlan p;
     bool fits = false;
@@ -851,11 +880,10 @@ void choose_form(spmv_matrix A, CgWorkspace& w) {
   }
   std::vector<FusedPlan> plans;
   {
-    FusedPlan p1, p2, p3;
+    FusedPlan p1, p2, p3, p4;
     if (plan_fused<CgFusedOne, true>(A, sp, p1)) plans.push_back(std::move(p1));
     if (plan_fused<CgFusedTwo, true>(A, sp, p2)) plans.push_back(std::move(p2));
     if (plan_fused<CgFusedTwoDeep, false>(A, sp, p3)) plans.push_back(std::move(p3));
-    FusedPlan p4;
     if (plan_fused<CgFusedThree, false>(A, sp, p4)) plans.push_back(std::move(p4));
   }
   if (plans.empty()) return;

@@ -16,15 +16,15 @@ pytestmark = pytest.mark.gpu
 PLANS = ["1:smem", "2:smem", "1:global", "2:global", "3:global"]
 
 
-def setup(monkeypatch, plan, W, P, width=8):
+def setup(monkeypatch, plan, W, P, width=8, kernel="staged"):
     monkeypatch.setenv("SPMV_B200_CG_FUSED", plan)
     comm, cm, rm, M, D = build(W, P)
-    M.set_kernel("staged", width)
+    M.set_kernel(kernel, width)
     return comm, M, D
 
 
-def solve(monkeypatch, plan, W, P, width=8, max_its=10000):
-    comm, M, D = setup(monkeypatch, plan, W, P, width)
+def solve(monkeypatch, plan, W, P, width=8, max_its=10000, kernel="staged"):
+    comm, M, D = setup(monkeypatch, plan, W, P, width, kernel)
     b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(P)]
     x, k, info = S.cg(comm, M, b, max_its, W.rtol, info=True)
     xg = np.concatenate([x[q][:D.local_sizes[q]] for q in range(P)])
@@ -133,3 +133,4 @@ def test_fused_with_an_empty_rank_and_unaligned_ranks(monkeypatch, cuda_device, 
     assert abs(k1 - k0) <= 2
     assert np.linalg.norm(x1 - x0) <= 1e-9 * np.linalg.norm(x0)
     assert true_relres(W, x1) < 1.5 * W.rtol
+
