@@ -633,6 +633,111 @@ def run_ours(args, info):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Per-configuration table (--table): the CPU restatement beside the GPU path
+# ---------------------------------------------------------------------------
+def run_table(args):
+    """For c1, c2, c3 and c5 at full size, one JSON line each and a markdown
+    table: SpMV GB/s (B_spmv over one L2GMap::update + Matrix::mult) and CG
+    solves/s, on the GPU (autotuned product; L2 flushed between SpMV reps
+    for the configurations that fit in L2) and for the oracle's restatement
+    on all host threads (SpMV: best of repeated update + mult; CG: a bounded
+    run of iterations scaled to the GPU's iteration count)."""
+    import torch
+    import spmv_b200 as S
+    import oracle
+    from spmv_b200 import gen
+    nth = oracle.max_threads()
+    dev = torch.device("cuda:0")
+    flush = torch.ones(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    rows = []
+    for name in ("c1", "c2", "c3", "c5"):
+        W = gen.workload(name)
+        D = gen.distribute(W.A, W.P)
+        P, n, nnz = W.P, W.A.nrows, W.A.nnz
+        g = int(sum(len(x) for x in D.ghosts))
+        B = spmv_bytes(n, nnz, P, g)
+        comm = S.Comm(size=P, device=0)
+        cm = S.L2GMap(comm, D.local_sizes, D.ghosts)
+        rm = S.L2GMap(comm, D.local_sizes, [[] for _ in range(P)])
+        M = S.Matrix(comm, D.blocks, cm, rm)
+        M.autotune(reps=10)
+        stream = torch.cuda.ExternalStream(comm.stream, device=dev)
+        resident = B < 100e6
+        xs = [torch.rand(cm.vec_len(q), dtype=torch.float64, device=dev) for q in range(P)]
+        ys = [torch.empty(D.local_sizes[q], dtype=torch.float64, device=dev) for q in range(P)]
+        for _ in range(3):
+            cm.update(xs)
+            M.mult(xs, out=ys)
+        # Reps queued behind a spin kernel, so the host has issued all of
+        # them before the first runs; each rep's update + mult is bracketed
+        # by its own events (GPU time alone).  For the L2-resident
+        # configurations each rep follows a read of 256 MB, which leaves the
+        # L2 holding other, clean lines.
+        R = 50
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(R)]
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            torch.cuda._sleep(200_000_000)  # ~0.1 s at B200 clocks
+            for i in range(R):
+                if resident:
+                    flush.sum(dtype=torch.int64)
+                ev[i][0].record(stream)
+                cm.update(xs)
+                M.mult(xs, out=ys)
+                ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        times = [a.elapsed_time(b) / 1e3 for a, b in ev]
+        gpu_spmv = B / statistics.median(times) / 1e9
+        # GPU CG: device-resident b and x, the configuration's tolerance.
+        bd = [torch.from_numpy(W.b[D.ranges[q]:D.ranges[q + 1]].copy()).to(dev)
+              for q in range(P)]
+        xd = [torch.zeros(cm.vec_len(q), dtype=torch.float64, device=dev) for q in range(P)]
+        _, k = S.cg(comm, M, bd, 20000, W.rtol, x=xd)
+        reps = 3 if n < 3_000_000 else 1
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            S.cg(comm, M, bd, 20000, W.rtol, x=xd)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        gpu_cg = reps / (e0.elapsed_time(e1) / 1e3)
+        # CPU restatement: update + mult over all ranks, then a CG sample.
+        om = oracle.Map(D.local_sizes, D.ghosts)
+        xh = [np.random.default_rng(q).uniform(-1, 1, cm.vec_len(q)) for q in range(P)]
+        cpu_t = []
+        t_end = time.perf_counter() + min(5.0, args.cpu_budget)
+        while time.perf_counter() < t_end or len(cpu_t) < 3:
+            t0 = time.perf_counter()
+            om.update(xh)
+            for q in range(P):
+                rp, ci, va = D.blocks[q]
+                oracle.csr_mult(rp, ci, va, xh[q], nthreads=nth)
+            cpu_t.append(time.perf_counter() - t0)
+        cpu_spmv = B / min(cpu_t) / 1e9
+        spi, kk = cpu_sample(W, D, args.cpu_budget, nth)
+        cpu_cg = 1.0 / (spi * k)
+        row = {"config": name, "n": n, "nnz": nnz, "ranks": P, "cg_iterations": int(k),
+               "cg_form": list(M.cg_form()), "mult_kernel": list(M.get_kernel()),
+               "cpu_spmv_gbs": cpu_spmv, "cpu_cg_solves_per_s": cpu_cg, "cpu_threads": nth,
+               "cpu_cg_sample_iterations": kk, "gpu_spmv_gbs": gpu_spmv,
+               "gpu_cg_solves_per_s": gpu_cg, "l2": "flushed" if resident else "exceeded"}
+        rows.append(row)
+        print(json.dumps(row), flush=True)
+        M.close()
+        cm.close()
+        rm.close()
+        comm.close()
+    print("| cfg | CPU SpMV GB/s | CPU CG solves/s | cores | GPU SpMV GB/s | GPU CG solves/s |")
+    print("|---|---|---|---|---|---|")
+    for r in rows:
+        print("| %s | %.1f | %.4g | %d | %.0f | %.4g |" % (
+            r["config"], r["cpu_spmv_gbs"], r["cpu_cg_solves_per_s"], r["cpu_threads"],
+            r["gpu_spmv_gbs"], r["gpu_cg_solves_per_s"]))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -647,12 +752,18 @@ def main():
                     help="skip the c3/c4/c5 mixed, batched and adjoint measurements")
     ap.add_argument("--extra-reps", type=int, default=2)
     ap.add_argument("--c4-count", type=int, default=256)
+    ap.add_argument("--table", action="store_true",
+                    help="per-configuration CPU/GPU table (c1, c2, c3, c5) instead of the "
+                         "benchmark line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     info = dist_init()
     try:
-        if args.impl == "reference":
+        if args.table:
+            if info.rank == 0:
+                run_table(args)
+        elif args.impl == "reference":
             run_reference(args, info.world, info.rank)
         else:
             run_ours(args, info)
