@@ -11,6 +11,8 @@
 // tile), so the grid is sized to the GPU rather than to the matrix.  W follows
 // the mean row length so that one pass of 16-byte loads covers a typical row.
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 #include <cmath>
 
 #include "internal.h"
@@ -176,6 +178,19 @@ SolverProduct choose_solver_product(spmv_matrix A, spmv_dtype dt, const void* x,
     }
   }
   require(!cands.empty(), "spmv: no product kernel applies to this matrix");
+  // SPMV_B200_SOLVER_PRODUCT=<vector|sell|staged>:<width>:<16|32> keeps only that
+  // candidate (for profilers, whose serialised replays distort the timing).
+  if (const char* pin = std::getenv("SPMV_B200_SOLVER_PRODUCT")) {
+    static const char* kinds[] = {"vector", "sell", "staged"};
+    std::vector<SolverProduct> kept;
+    for (const SolverProduct& cd : cands) {
+      const std::string name = std::string(kinds[int(cd.kind)]) + ":" + std::to_string(cd.w) +
+                               ":" + (cd.d16 ? "16" : "32");
+      if (name == pin) kept.push_back(cd);
+    }
+    require(!kept.empty(), "spmv: SPMV_B200_SOLVER_PRODUCT names no candidate of this matrix");
+    cands = kept;
+  }
 
   const spmv_l2gmap rm = A->row_map;
   std::vector<const void*> xs(P), own(P);
