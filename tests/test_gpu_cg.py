@@ -193,3 +193,19 @@ def test_solver_product_needs_a_solve(cuda_device):
         M.solver_product("cg")
     with pytest.raises(S.SpmvError, match="has not run"):
         M.solver_product("mixed32")
+
+
+def test_solver_product_pin(cuda_device, monkeypatch):
+    """SPMV_B200_SOLVER_PRODUCT keeps one product candidate (for profilers);
+    a pin that names none of the matrix's candidates is refused."""
+    W = gen.workload("c2", 24)
+    monkeypatch.setenv("SPMV_B200_SOLVER_PRODUCT", "sell:4:32")
+    comm, cm, rm, M, D = build(W, 2)
+    b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(2)]
+    x, k = S.cg(comm, M, b, 10000, W.rtol)
+    assert M.solver_product("cg")[:3] == ("sell", 4, 32)
+    monkeypatch.setenv("SPMV_B200_SOLVER_PRODUCT", "sell:3:32")
+    comm2, cm2, rm2, M2, D2 = build(W, 2)
+    with pytest.raises(S.SpmvError) as e:
+        S.cg(comm2, M2, b, 10000, W.rtol)
+    assert "SPMV_B200_SOLVER_PRODUCT" in str(e.value)
