@@ -134,3 +134,21 @@ def test_fused_with_an_empty_rank_and_unaligned_ranks(monkeypatch, cuda_device, 
     assert np.linalg.norm(x1 - x0) <= 1e-9 * np.linalg.norm(x0)
     assert true_relres(W, x1) < 1.5 * W.rtol
 
+
+
+@pytest.mark.parametrize("plan", ["2:smem", "3:global"])
+def test_fused_after_set_values(monkeypatch, cuda_device, plan):
+    """New values on the same pattern reach the fused solve (its workspace
+    keeps its plan and product).  Scaling A by 4 scales every product, alpha
+    and x exactly in binary floating point, so the solve of 4A gives x/4 bit
+    for bit in the same iterations."""
+    W = gen.workload("c2", 32)
+    monkeypatch.setenv("SPMV_B200_D16", "0")
+    comm, M, D = setup(monkeypatch, plan, W, 8, 7)
+    b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(8)]
+    x1, k1 = S.cg(comm, M, b, 10000, W.rtol)
+    M.set_values([va * 4.0 for (rp, ci, va) in D.blocks])
+    x2, k2 = S.cg(comm, M, b, 10000, W.rtol)
+    assert M.cg_form()[0] == "fused"
+    assert k2 == k1
+    assert all(np.array_equal(a * 4.0, c) for a, c in zip(x2, x1))
