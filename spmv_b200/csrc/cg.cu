@@ -96,6 +96,7 @@ struct CgPtrs {
   int ntiles;
   unsigned long long* bar;  // fused solve: grid barrier counter
   double* partials2;        // fused solve: second reduction's partials
+  unsigned long long wait_ns;  // fused solve: bound of each grid wait
 };
 
 __global__ void __launch_bounds__(EW_BS)
@@ -295,7 +296,8 @@ __device__ __forceinline__ bool cg_fused_solve(const CgPtrs& c, const FusedCta& 
                                                Product&& product) {
   const int tid = int(threadIdx.x);
   auto grid_sum = [&](double v, double* parts, unsigned long long epoch, double* total) {
-    return coop_grid_sum<NT>(v, parts, c.bar, epoch * gridDim.x, &c.st->stage_err, gs, total);
+    return coop_grid_sum<NT>(v, parts, c.bar, epoch * gridDim.x, &c.st->stage_err, c.wait_ns,
+                             gs, total);
   };
   // Init: r = p = b, x = 0, rnorm0 = b.b.  Barrier epochs: 1 for the init,
   // 3j+2, 3j+3, 3j+4 for phases A, B, C of iteration j.
@@ -413,7 +415,7 @@ __device__ __forceinline__ bool cg_fused_solve(const CgPtrs& c, const FusedCta& 
       if (!go) break;
     }
     if (!coop_grid_barrier<NT>(c.bar, (3ull * unsigned(k) + 1) * gridDim.x, &c.st->stage_err,
-                               gs)) {
+                               c.wait_ns, gs)) {
       ok = false;
       break;
     }
@@ -584,6 +586,12 @@ CgPtrs cg_ptrs(CgWorkspace& w) {
   c.ntiles = w.ntiles;
   c.bar = w.bar.as<unsigned long long>();
   c.partials2 = w.partials2.as<double>();
+  // Bound of the fused solve's grid waits: 2 s (a healthy wait is
+  // microseconds); SPMV_B200_WAIT_LIMIT_NS overrides it (tests make it run
+  // out on purpose).
+  c.wait_ns = 2000000000ull;
+  if (const char* lim = std::getenv("SPMV_B200_WAIT_LIMIT_NS"))
+    c.wait_ns = std::strtoull(lim, nullptr, 10);
   return c;
 }
 
@@ -999,7 +1007,7 @@ void cg_run(spmv_matrix A, int max_its, double rtol, spmv_cg_info* info) {
                              cudaMemcpyDeviceToHost, s));
   SPMVB_CUDA(cudaStreamSynchronize(s));
   if (w.host.stage_err)
-    fail(SPMV_ERROR_CUDA, "spmv::cg - a staged product's bounded wait timed out");
+    fail(SPMV_ERROR_CUDA, "spmv::cg - a bounded wait on the device timed out");
   if (info) {
     info->iterations = w.host.k;
     info->status = w.host.status;

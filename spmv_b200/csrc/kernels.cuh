@@ -298,9 +298,10 @@ __device__ __forceinline__ bool grid_sum2(double a, double b, double* partials,
 // Grid barrier and grid sum for cooperative launches (every CTA resident),
 // over the first NT threads of each CTA (named barrier 1; the CTA's other
 // warps do not take part).  `count` is zero at launch; the e-th barrier of
-// the launch waits for count = e * gridDim.x.  Waits are bounded: a barrier
-// that does not complete, or sees *err raised, raises *err and returns false
-// (CTAs that have already passed fail at their next barrier).
+// the launch waits for count = e * gridDim.x.  Waits are bounded by
+// `limit_ns` of global time: a barrier that does not complete in time, or
+// sees *err raised, raises *err and returns false (CTAs that have already
+// passed fail at their next barrier).
 __device__ __forceinline__ void named_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
@@ -309,13 +310,19 @@ __device__ __forceinline__ void named_sync(int id, int nthreads) {
 // writes before the barrier are visible to any CTA that sees the count),
 // the wait an acquire.
 __device__ __forceinline__ bool grid_arrive_wait(unsigned long long* count,
-                                                 unsigned long long target, int* err) {
+                                                 unsigned long long target, int* err,
+                                                 unsigned long long limit_ns) {
   asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(count), "l"(1ull) : "memory");
-  for (uint32_t i = 0; i < (1u << 23); ++i) {
+  unsigned long long t0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (uint32_t i = 0;; ++i) {
     unsigned long long c;
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(c) : "l"(count) : "memory");
     if (c >= target) return true;
     if (*static_cast<volatile int*>(err)) return false;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 > limit_ns) break;
     if (i >= 64) __nanosleep(32);
   }
   atomicExch(err, 1);
@@ -333,9 +340,9 @@ struct GridSum {
 template <int NT>
 __device__ __forceinline__ bool coop_grid_barrier(unsigned long long* count,
                                                   unsigned long long target, int* err,
-                                                  GridSum<NT>& s) {
+                                                  unsigned long long limit_ns, GridSum<NT>& s) {
   named_sync(1, NT);
-  if (threadIdx.x == 0) s.ok = grid_arrive_wait(count, target, err);
+  if (threadIdx.x == 0) s.ok = grid_arrive_wait(count, target, err, limit_ns);
   named_sync(1, NT);
   return s.ok != 0;
 }
@@ -366,11 +373,12 @@ __device__ __forceinline__ double sum_partials(const GridSum<NT>& s) {
 template <int NT>
 __device__ __forceinline__ bool coop_grid_sum(double v, double* parts, unsigned long long* count,
                                               unsigned long long target, int* err,
-                                              GridSum<NT>& s, double* total) {
+                                              unsigned long long limit_ns, GridSum<NT>& s,
+                                              double* total) {
   warp_partials<NT>(v, s);
   if (threadIdx.x == 0) {
     __stcg(parts + blockIdx.x, sum_partials<NT>(s));
-    s.ok = grid_arrive_wait(count, target, err);
+    s.ok = grid_arrive_wait(count, target, err, limit_ns);
   }
   named_sync(1, NT);
   if (!s.ok) return false;

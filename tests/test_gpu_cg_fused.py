@@ -152,3 +152,22 @@ def test_fused_after_set_values(monkeypatch, cuda_device, plan):
     assert M.cg_form()[0] == "fused"
     assert k2 == k1
     assert all(np.array_equal(a * 4.0, c) for a, c in zip(x2, x1))
+
+
+def test_fused_wait_limit_reports_an_error(monkeypatch, cuda_device):
+    """The fused solve's grid waits are bounded: with the bound at 1 ns every
+    CTA that has to wait gives up at once, raises the device's error flag and
+    leaves, and the host reports the timeout.  The context stays usable: the
+    same matrix then solves with the default bound."""
+    W = gen.workload("c2", 32)
+    comm, M, D = setup(monkeypatch, "2:smem", W, 8, 7)
+    b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(8)]
+    monkeypatch.setenv("SPMV_B200_WAIT_LIMIT_NS", "1")
+    with pytest.raises(S.SpmvError) as e:
+        S.cg(comm, M, b, 10000, W.rtol)
+    assert "timed out" in str(e.value)
+    monkeypatch.delenv("SPMV_B200_WAIT_LIMIT_NS")
+    x, k, info = S.cg(comm, M, b, 10000, W.rtol, info=True)
+    assert M.cg_form()[0] == "fused" and info.status == 0 and k > 0
+    xg = np.concatenate([x[q][:D.local_sizes[q]] for q in range(8)])
+    assert true_relres(W, xg) < 1.5 * W.rtol
