@@ -322,6 +322,13 @@ int spmv_matrix_solver_product(spmv_matrix A, int solver, spmv_kernel* kernel,
  * Fails when spmv_cg has not run on the matrix.  No reference counterpart. */
 int spmv_matrix_cg_form(spmv_matrix A, int* fused, int* ctas_per_sm, int* r_shared);
 
+/* The same for spmv_cg_mixed: *fused = 0 for its CUDA graph (three kernels
+ * per inner iteration, three more per refinement), 1 for one cooperative
+ * launch per solve (the FP32 residual in shared memory when *r_shared = 1).
+ * Fails when spmv_cg_mixed has not run on the matrix.  No reference
+ * counterpart. */
+int spmv_matrix_cg_mixed_form(spmv_matrix A, int* fused, int* ctas_per_sm, int* r_shared);
+
 typedef struct spmv_ir_info {
   int iterations;   /* inner FP32 CG iterations                             */
   int refinements;  /* FP64 true-residual recomputations                    */

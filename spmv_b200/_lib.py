@@ -116,6 +116,7 @@ _SIGS = {
     "spmv_batch_solve": [_p, _int, _pp, _pp, _int, C.c_double, C.POINTER(IrInfo)],
     "spmv_matrix_autotune": [_p, _int, C.POINTER(TuneResult)],
     "spmv_matrix_cg_form": [_p, C.POINTER(_int), C.POINTER(_int), C.POINTER(_int)],
+    "spmv_matrix_cg_mixed_form": [_p, C.POINTER(_int), C.POINTER(_int), C.POINTER(_int)],
     "spmv_matrix_solver_product": [_p, _int, C.POINTER(_int), C.POINTER(_int),
                                    C.POINTER(_int), C.POINTER(C.c_double)],
     "spmv_matrix_mult_block": [_p, _int, _int, _pp, _pp],

@@ -344,13 +344,15 @@ class Matrix:
              C.byref(bits), C.byref(us))
         return _lib.KERNEL_NAMES[k.value], w.value, bits.value, us.value
 
-    def cg_form(self):
-        """How cg runs on this matrix: ("graph", 0, None) for three kernels
-        per iteration in a CUDA graph, or ("fused", CTAs per SM, "smem" or
-        "global": where the residual lives) for one cooperative launch per
-        solve; fails if cg has not run on the matrix."""
+    def cg_form(self, solver="cg"):
+        """How cg (solver="cg") or cg_mixed (solver="mixed") runs on this
+        matrix: ("graph", 0, None) for its kernels in a CUDA graph, or
+        ("fused", CTAs per SM, "smem" or "global": where the residual lives)
+        for one cooperative launch per solve; fails if that solver has not
+        run on the matrix."""
+        fn = {"cg": "spmv_matrix_cg_form", "mixed": "spmv_matrix_cg_mixed_form"}[solver]
         f, cps, rs = C.c_int(), C.c_int(), C.c_int()
-        call("spmv_matrix_cg_form", self._h, C.byref(f), C.byref(cps), C.byref(rs))
+        call(fn, self._h, C.byref(f), C.byref(cps), C.byref(rs))
         if not f.value:
             return "graph", 0, None
         return "fused", cps.value, "smem" if rs.value else "global"

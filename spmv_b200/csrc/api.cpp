@@ -1002,4 +1002,15 @@ int spmv_matrix_cg_form(spmv_matrix A, int* fused, int* ctas_per_sm, int* r_shar
   });
 }
 
+int spmv_matrix_cg_mixed_form(spmv_matrix A, int* fused, int* ctas_per_sm, int* r_shared) {
+  return guard([&] {
+    check_mat(A);
+    require(fused && ctas_per_sm && r_shared, "spmv: NULL output");
+    const CgForm f = ir_form(A);
+    *fused = f.fused ? 1 : 0;
+    *ctas_per_sm = f.cps;
+    *r_shared = f.rs ? 1 : 0;
+  });
+}
+
 }  // extern "C"

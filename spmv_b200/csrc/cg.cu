@@ -250,11 +250,6 @@ __global__ void __launch_bounds__(EW_BS) cg_update_xp(const CgPtrs c) {
 // ever read it), so it never crosses HBM.  The arithmetic of every vector
 // element is the graph form's; the two dot products are summed in a
 // different grouping (per-CTA partials over the CTA's rows).
-struct FusedCta {
-  int32_t t0, t1;  // tiles [t0, t1)
-  int32_t g0, g1;  // global rows [g0, g1)
-};
-
 // Phase A of the fused solve for one consumer thread: one pass of the staged
 // traversal, y = A p, returning this thread's share of p.y.
 template <class CFG, int U, typename CI>
@@ -586,12 +581,7 @@ CgPtrs cg_ptrs(CgWorkspace& w) {
   c.ntiles = w.ntiles;
   c.bar = w.bar.as<unsigned long long>();
   c.partials2 = w.partials2.as<double>();
-  // Bound of the fused solve's grid waits: 2 s (a healthy wait is
-  // microseconds); SPMV_B200_WAIT_LIMIT_NS overrides it (tests make it run
-  // out on purpose).
-  c.wait_ns = 2000000000ull;
-  if (const char* lim = std::getenv("SPMV_B200_WAIT_LIMIT_NS"))
-    c.wait_ns = std::strtoull(lim, nullptr, 10);
+  c.wait_ns = fused_wait_ns();
   return c;
 }
 
@@ -682,78 +672,6 @@ void build_graph(spmv_matrix A, CgWorkspace& w) {
   SPMVB_CUDA(cudaGraphInstantiate(&w.exec, w.graph, 0));
 }
 
-// Fused solve plans.  The tiles are split into `grid` contiguous runs of
-// about n / grid rows each (tile starts are row boundaries, so each run
-// covers a contiguous range of global rows); returns the longest run.
-int64_t fused_ctas(spmv_matrix A, const DevCsr::StagedTable& t, int grid,
-                   std::vector<FusedCta>& out) {
-  const std::vector<int64_t>& ranges = A->row_map->ranges;
-  const int T = t.ntiles;
-  const int64_t n = ranges.back();
-  std::vector<int64_t> start(size_t(T) + 1);
-  for (int k = 0; k < T; ++k) {
-    const DevCsr::StagedTable::Rows& r = t.rows[size_t(k)];
-    start[size_t(k)] =
-        std::min<int64_t>(ranges[size_t(r.rank)] + int64_t(r.s0) * 32, ranges[size_t(r.rank) + 1]);
-  }
-  start[size_t(T)] = n;
-  out.assign(size_t(grid), FusedCta{});
-  int kb = 0;
-  int64_t longest = 0;
-  for (int b = 0; b < grid; ++b) {
-    const int64_t target = n * (b + 1) / grid;
-    const int ke = b + 1 == grid
-                       ? T
-                       : int(std::lower_bound(start.begin() + kb, start.end(), target) -
-                             start.begin());
-    out[size_t(b)] = {kb, ke, int32_t(start[size_t(kb)]), int32_t(start[size_t(ke)])};
-    longest = std::max(longest, start[size_t(ke)] - start[size_t(kb)]);
-    kb = ke;
-  }
-  return longest;
-}
-
-struct FusedPlan {
-  const void* fn = nullptr;
-  int grid = 0, block = 0, smem = 0;
-  int cps = 0;      // CTAs per SM
-  bool rs = false;  // r in shared memory
-  std::vector<FusedCta> ctas;
-};
-
-// A plan for kernel `fn` of `block` threads at `cps` CTAs per SM, with
-// `stage_smem` bytes of stage buffers and r in shared memory (rs) or global
-// memory; false when it does not fit.
-bool plan_common(spmv_matrix A, const SolverProduct& sp, const void* fn, int block, int cps,
-                 int64_t stage_smem, bool rs, FusedPlan& plan) {
-  if (!fn) return false;
-  const DevCsr::StagedTable& t = cg_tiles(A, sp);
-  if (!t.ok) return false;
-  spmv_comm comm = A->comm;
-  const int grid = std::max(1, comm->num_sms) * cps;
-  std::vector<FusedCta> ctas;
-  const int64_t longest = fused_ctas(A, t, grid, ctas);
-  const int64_t smem = stage_smem + (rs ? (longest * 8 + 15) / 16 * 16 : 0);
-  int optin = 0;
-  SPMVB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
-                                    comm->device));
-  cudaFuncAttributes fa{};
-  SPMVB_CUDA(cudaFuncGetAttributes(&fa, fn));
-  if (smem + int64_t(fa.sharedSizeBytes) > optin) return false;
-  SPMVB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  int nb = 0;
-  SPMVB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, size_t(smem)));
-  if (nb < cps) return false;
-  plan.fn = fn;
-  plan.grid = grid;
-  plan.block = block;
-  plan.smem = int(smem);
-  plan.cps = cps;
-  plan.rs = rs;
-  plan.ctas = std::move(ctas);
-  return true;
-}
-
 // Staged product: shape CFG (CFG::MINB CTAs per SM).
 template <class CFG, bool RS>
 bool plan_fused(spmv_matrix A, const SolverProduct& sp, FusedPlan& plan) {
@@ -761,8 +679,8 @@ bool plan_fused(spmv_matrix A, const SolverProduct& sp, FusedPlan& plan) {
                     CFG::max_entries(12) == SolverStaged::max_entries(12),
                 "fused shapes use the solver product's tiles");
   const int eb = 8 + (sp.d16 ? 2 : 4);
-  return plan_common(A, sp, (const void*)fused_fn<CFG, RS>(sp), CFG::BS, CFG::MINB,
-                     CFG::smem_bytes(eb), RS, plan);
+  return fused_plan(A, cg_tiles(A, sp), (const void*)fused_fn<CFG, RS>(sp), CFG::BS, CFG::MINB,
+                    CFG::smem_bytes(eb), RS ? 8 : 0, plan);
 }
 
 void use_plan(CgWorkspace& w, FusedPlan& plan) {
@@ -916,6 +834,75 @@ void choose_form(spmv_matrix A, CgWorkspace& w) {
 }
 
 }  // namespace
+
+// Fused solve plans.  The tiles are split into `grid` contiguous runs of
+// about n / grid rows each (tile starts are row boundaries, so each run
+// covers a contiguous range of global rows); returns the longest run.
+int64_t fused_ctas(spmv_matrix A, const DevCsr::StagedTable& t, int grid,
+                   std::vector<FusedCta>& out) {
+  const std::vector<int64_t>& ranges = A->row_map->ranges;
+  const int T = t.ntiles;
+  const int64_t n = ranges.back();
+  std::vector<int64_t> start(size_t(T) + 1);
+  for (int k = 0; k < T; ++k) {
+    const DevCsr::StagedTable::Rows& r = t.rows[size_t(k)];
+    start[size_t(k)] =
+        std::min<int64_t>(ranges[size_t(r.rank)] + int64_t(r.s0) * 32, ranges[size_t(r.rank) + 1]);
+  }
+  start[size_t(T)] = n;
+  out.assign(size_t(grid), FusedCta{});
+  int kb = 0;
+  int64_t longest = 0;
+  for (int b = 0; b < grid; ++b) {
+    const int64_t target = n * (b + 1) / grid;
+    const int ke = b + 1 == grid
+                       ? T
+                       : int(std::lower_bound(start.begin() + kb, start.end(), target) -
+                             start.begin());
+    out[size_t(b)] = {kb, ke, int32_t(start[size_t(kb)]), int32_t(start[size_t(ke)])};
+    longest = std::max(longest, start[size_t(ke)] - start[size_t(kb)]);
+    kb = ke;
+  }
+  return longest;
+}
+
+
+bool fused_plan(spmv_matrix A, const DevCsr::StagedTable& t, const void* fn, int block,
+                int cps, int64_t stage_smem, int rs_bytes, FusedPlan& plan) {
+  if (!fn || !t.ok) return false;
+  spmv_comm comm = A->comm;
+  const int grid = std::max(1, comm->num_sms) * cps;
+  std::vector<FusedCta> ctas;
+  const int64_t longest = fused_ctas(A, t, grid, ctas);
+  const int64_t smem = stage_smem + (longest * rs_bytes + 15) / 16 * 16;
+  int optin = 0;
+  SPMVB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                    comm->device));
+  cudaFuncAttributes fa{};
+  SPMVB_CUDA(cudaFuncGetAttributes(&fa, fn));
+  if (smem + int64_t(fa.sharedSizeBytes) > optin) return false;
+  SPMVB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  int nb = 0;
+  SPMVB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, size_t(smem)));
+  if (nb < cps) return false;
+  plan.fn = fn;
+  plan.grid = grid;
+  plan.block = block;
+  plan.smem = int(smem);
+  plan.cps = cps;
+  plan.rs = rs_bytes > 0;
+  plan.ctas = std::move(ctas);
+  return true;
+}
+
+// A healthy grid wait is microseconds; tests set the limit low to make one
+// run out on purpose.
+unsigned long long fused_wait_ns() {
+  unsigned long long ns = 2000000000ull;
+  if (const char* lim = std::getenv("SPMV_B200_WAIT_LIMIT_NS"))
+    ns = std::strtoull(lim, nullptr, 10);
+  return ns;
+}
 
 void destroy_cg_workspace(CgWorkspace* w) { delete w; }
 

@@ -373,6 +373,30 @@ using ProductLauncher =
 // and width.
 SolverProduct choose_solver_product(spmv_matrix A, spmv_dtype dt, const void* x, void* y,
                                     bool xown_rows, const ProductLauncher& launch);
+// Fused (cooperative, persistent) solver kernels: each CTA owns a contiguous
+// run of a staged tile table and so a contiguous range of global rows.
+struct FusedCta {
+  int32_t t0, t1;  // tiles [t0, t1)
+  int32_t g0, g1;  // global rows [g0, g1)
+};
+// Splits the tiles of `t` into `grid` contiguous runs of about n / grid rows
+// each; returns the longest run's row count.
+int64_t fused_ctas(spmv_matrix A, const DevCsr::StagedTable& t, int grid,
+                   std::vector<FusedCta>& out);
+struct FusedPlan {
+  const void* fn = nullptr;
+  int grid = 0, block = 0, smem = 0;
+  int cps = 0;      // CTAs per SM
+  bool rs = false;  // a vector of the CTA's rows kept in shared memory
+  std::vector<FusedCta> ctas;
+};
+// A plan for kernel `fn` of `block` threads at `cps` CTAs per SM over the
+// tiles of `t`: `stage_smem` bytes of stage buffers plus `rs_bytes` per row
+// of the longest run in shared memory; false when it does not fit.
+bool fused_plan(spmv_matrix A, const DevCsr::StagedTable& t, const void* fn, int block,
+                int cps, int64_t stage_smem, int rs_bytes, FusedPlan& plan);
+// Bound of each grid wait of a fused solve: 2 s, or SPMV_B200_WAIT_LIMIT_NS.
+unsigned long long fused_wait_ns();
 // The products chosen by the built solver workspaces (fails if none).
 SolverProduct cg_product(spmv_matrix A);
 // How the built CG workspace runs a solve (fails if none).
@@ -382,6 +406,7 @@ struct CgForm {
   bool rs = false;
 };
 CgForm cg_form(spmv_matrix A);
+CgForm ir_form(spmv_matrix A);  // spmv_cg_mixed's
 SolverProduct ir_product(spmv_matrix A, bool fp32);
 // Builds the SELL copies the solvers may time (when SELL is applicable).
 void prepare_solver_layouts(spmv_matrix A, bool fp32);

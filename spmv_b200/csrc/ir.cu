@@ -24,6 +24,8 @@
 // refinement; IF(refine) { fold x; FP64 residual; resync r, p.r } ; K3 p }.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <string>
 
 #include <type_traits>
 
@@ -48,6 +50,13 @@ struct IrWorkspace {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaGraphConditionalHandle h_loop = 0, h_ref = 0;
+  // Fused form (one cooperative launch per solve), when chosen.
+  bool fused = false;
+  const void* fused_fn = nullptr;
+  int fused_grid = 0, fused_block = 0, fused_smem = 0;
+  bool fused_rs = false;
+  spmvb::DevBuf bar, fpartials, ctas;
+  spmvb::SpmvArgs fa32, fa64;  // FP32 product over p, FP64 SELL over x
   IrState host{};
   ~IrWorkspace() {
     if (exec) spmvb::soft_check(cudaGraphExecDestroy(exec), "cudaGraphExecDestroy");
@@ -75,6 +84,8 @@ struct IrPtrs {
   const StagedDesc* tiles32;  // staged products only
   const StagedDesc* tiles64;
   int ntiles32, ntiles64;
+  unsigned long long* bar;     // fused solve: grid barrier counter
+  unsigned long long wait_ns;  // fused solve: bound of each grid wait
 };
 
 #define IR_LOOP(i)                                                      \
@@ -311,6 +322,360 @@ __global__ void __launch_bounds__(EW)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fused solve: the whole mixed-precision CG (init, inner iterations and the
+// refinements) as one cooperative launch of persistent CTAs, each owning a
+// contiguous run of the FP32 product's staged tiles and so a contiguous
+// range of global rows; grid barriers between the phases.  Per inner
+// iteration, with exactly the graph form's arithmetic:
+//
+//   A  y = A32 p (the staged FP32 traversal), p.y in FP64  -> alpha
+//   B  r -= alpha y, r.r; the refinement test              -> beta ...
+//   (refining: x += d + alpha p, d = 0 -> barrier; r = fl32(b - A x) with
+//    the FP64 product over the CTA's slices (SELL-32 from global memory,
+//    storage order); ||b - A x||, r.r, r.p                  -> beta, c)
+//   C  d += alpha p (unless refined), p = r + beta (p - c r) -> barrier
+//
+// RS: the CTA's rows of r (FP32) stay in shared memory for the whole solve.
+// The refinement's FP64 residual is written straight into r (the graph form
+// keeps it in r64 first: the same values).
+struct IrScalars {
+  double rr0, rr, rr_new, rr_max, alpha, beta, pap, c, rtol2, delta2, rr_true, rr_prev;
+  int k, kmax, status, converged, refine, refinements, k_guard, go;
+};
+
+// Phase A for one consumer thread: returns its share of p.y.
+template <class CFG, int U, typename CI>
+__device__ __forceinline__ double ir_fused_product(const SpmvArgs& a, int count, uint64_t q_base,
+                                                   StagedLoop<CFG>& pipe,
+                                                   const unsigned char* smem, int* err,
+                                                   float* __restrict__ y,
+                                                   const float* __restrict__ p) {
+  const uint64_t keep = l2_policy_keep();
+  double acc = 0.0;
+  staged_loop_consume<CFG, float, CI, U>(
+      a, count, q_base, pipe, smem, err,
+      [&](const PartArg& P, int row, float sum) {
+        const int g = P.row0 + row;
+        st_pol(y + g, sum, keep);
+        acc += double(ld_pol(p + g, keep)) * double(sum);
+      },
+      XGather<float, true>());
+  return acc;
+}
+
+// The refinement's FP64 residual over the CTA's slices (tiles t0..t1 of
+// the FP32 table: the same slices in the FP64 SELL arrays), one warp per
+// slice, each row summed in storage order; f(g, r64) per row.
+template <int NW, bool D16, class F>
+__device__ __forceinline__ void ir_fused_residual(const SpmvArgs& a,
+                                                  const StagedDesc* __restrict__ tiles, int t0,
+                                                  int t1, const double* __restrict__ x,
+                                                  const double* __restrict__ b, F&& f) {
+  using CI = typename std::conditional<D16, int16_t, int32_t>::type;
+  constexpr int U = 4;
+  const int warp = int(threadIdx.x) >> 5, lane = int(threadIdx.x) & 31;
+  int q = warp;
+  for (int t = t0; t < t1; ++t) {
+    const StagedDesc* d = tiles + t;
+    const int ns = __ldg(&d->nslices);
+    if (q >= ns) {
+      q -= ns;
+      continue;
+    }
+    const PartArg& P = a.part[__ldg(&d->rank)];
+    const int s0 = __ldg(&d->s0);
+    const int32_t* __restrict__ soff = P.rowptr;
+    const CI* __restrict__ cols = reinterpret_cast<const CI*>(P.cols);
+    const double* __restrict__ vals = static_cast<const double*>(P.vals);
+    for (; q < ns; q += NW) {
+      const int slice = s0 + q;
+      const int o = __ldg(soff + slice);
+      const int w = (__ldg(soff + slice + 1) - o) >> 5;
+      const int row = slice * 32 + lane;
+      const int g = P.row0 + row;
+      double sum = 0.0;
+      for (int k0 = 0; k0 < w; k0 += U) {
+        double v[U], xv[U];
+        bool ok[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const bool in = k0 + u < w;
+          const int idx = o + (k0 + u) * 32 + lane;
+          const int ci = in ? int(cols[idx]) : 0;
+          ok[u] = in && (D16 ? ci != -32768 : ci >= 0);
+          v[u] = in ? vals[idx] : 0.0;
+          xv[u] = ok[u] ? x[D16 ? g + ci : ci] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (ok[u]) sum += v[u] * xv[u];
+      }
+      if (row < P.nrows) f(g, b[g] - sum);
+    }
+    q -= ns;
+  }
+}
+
+template <class CFG, int U, bool D16, bool RS>
+__global__ void __launch_bounds__(CFG::BS, CFG::MINB)
+    ir_fused(const __grid_constant__ SpmvArgs a32, const __grid_constant__ SpmvArgs a64,
+             const IrPtrs c, const FusedCta* __restrict__ ctas) {
+  using CI = typename std::conditional<D16, int16_t, int32_t>::type;
+  constexpr int NT = CFG::NC * 32;
+  constexpr int STAGES_BYTES = CFG::smem_bytes(4 + int(sizeof(CI)));
+  constexpr int V = 4;
+  extern __shared__ __align__(128) unsigned char staged_smem[];
+  __shared__ StagedLoop<CFG> pipe;
+  __shared__ GridSumN<NT, 1> gs1;
+  __shared__ GridSumN<NT, 2> gs2;
+  __shared__ GridSumN<NT, 3> gs3;
+  __shared__ GridSum<NT> gsb;
+  __shared__ FusedCta me;
+  __shared__ IrScalars sv;
+
+  const int tid = int(threadIdx.x);
+  if (tid == 0) {
+    me = ctas[blockIdx.x];
+    staged_loop_init(pipe);
+  }
+  __syncthreads();
+  int* err = &c.st->stage_err;
+  if (tid >= NT) {
+    if (tid == NT)
+      staged_loop_produce<CFG, float, CI>(a32, c.tiles32 + me.t0, me.t1 - me.t0, pipe,
+                                          staged_smem, err);
+    return;
+  }
+  auto r_at = [&](int g) -> float& {
+    return RS ? reinterpret_cast<float*>(staged_smem + STAGES_BYTES)[g - me.g0] : c.r[g];
+  };
+  // Grid syncs (sums and plain barriers) are numbered 1, 2, ...; sync e
+  // completes when the counter reaches e * gridDim.x.  A sum at sync e
+  // publishes into partial array e & 1 (3 per CTA): the array was last read
+  // before sync e - 1 at the latest, which every CTA has passed.
+  unsigned long long epoch = 0;
+  auto parts = [&](unsigned long long e) { return c.partials + (e & 1) * 3 * gridDim.x; };
+  auto sum1 = [&](double v, double& total) -> bool {
+    double in[1] = {v}, out[1] = {0.0};
+    ++epoch;
+    const bool okk = coop_grid_sum_n<NT, 1>(in, parts(epoch), c.bar, epoch * gridDim.x, err,
+                                            c.wait_ns, gs1, out);
+    total = out[0];
+    return okk;
+  };
+  auto barrier = [&]() {
+    ++epoch;
+    return coop_grid_barrier<NT>(c.bar, epoch * gridDim.x, err, c.wait_ns, gsb);
+  };
+  const uint64_t keep = l2_policy_keep();
+  bool ok = true;
+
+  // Init (ir_init): r = p = fl32(b), d = 0, x = 0; ||b||^2 and ||r||^2.
+  {
+    double bb = 0.0, rr = 0.0;
+    for (int g = me.g0 + tid; g < me.g1; g += NT) {
+      const double bi = c.b[g];
+      const float ri = float(bi);
+      r_at(g) = ri;
+      c.p[g] = ri;
+      c.d[g] = 0.0f;
+      c.x[g] = 0.0;
+      bb += bi * bi;
+      rr += double(ri) * double(ri);
+    }
+    double in[2] = {bb, rr}, out[2] = {0.0, 0.0};
+    ++epoch;
+    ok = coop_grid_sum_n<NT, 2>(in, parts(epoch), c.bar, epoch * gridDim.x, err, c.wait_ns,
+                                gs2, out);
+    if (tid == 0) {
+      sv.kmax = *static_cast<volatile int*>(&c.st->kmax);
+      sv.rtol2 = *static_cast<volatile double*>(&c.st->rtol2);
+      sv.delta2 = *static_cast<volatile double*>(&c.st->delta2);
+      sv.rr0 = out[0];
+      sv.rr = out[1];
+      sv.rr_max = out[1];
+      sv.rr_true = out[0];
+      sv.rr_new = sv.alpha = sv.beta = sv.pap = sv.rr_prev = 0.0;
+      sv.c = 0.0;
+      sv.k = sv.k_guard = sv.refinements = sv.refine = 0;
+      sv.status = SPMV_SUCCESS;
+      sv.converged = 0;
+      sv.go = ok && sv.kmax > 0 && out[0] > 0.0 && isfinite(out[0]);
+      if (!sv.go && ok) sv.converged = out[0] == 0.0 ? 1 : 0;
+    }
+    named_sync(1, NT);
+  }
+  int it = 0;
+  while (sv.go) {
+    // A (ir_spmv_dot): y = A32 p, p.y.
+    const int count = me.t1 - me.t0;
+    double pap = 0.0;
+    const bool okA = sum1(ir_fused_product<CFG, U, CI>(a32, count, uint64_t(it) * uint64_t(count),
+                                                        pipe, staged_smem, err, c.y, c.p),
+                          pap);
+    ++it;
+    if (!okA) {
+      ok = false;
+      break;
+    }
+    if (tid == 0) {
+      sv.pap = pap;
+      if (pap == 0.0 || !isfinite(pap)) sv.status = SPMV_ERROR_BREAKDOWN;
+      sv.alpha = sv.rr / pap;
+    }
+    named_sync(1, NT);
+    // B (ir_update): r -= alpha y, r.r; the refinement test.
+    const bool good = sv.status == SPMV_SUCCESS;
+    const float alpha32 = float(sv.alpha);
+    double acc = 0.0;
+    if (good) {
+      const int g1 = me.g1;
+      for (int g0 = me.g0 + tid; g0 < g1; g0 += V * NT) {
+        float yv[V];
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+          const int g = g0 + u * NT;
+          if (g < g1) yv[u] = ld_pol(c.y + g, keep);
+        }
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+          const int g = g0 + u * NT;
+          if (g < g1) {
+            const float ri = r_at(g) - alpha32 * yv[u];
+            r_at(g) = ri;
+            acc += double(ri) * double(ri);
+          }
+        }
+      }
+    }
+    double total = 0.0;
+    if (!sum1(acc, total)) {
+      ok = false;
+      break;
+    }
+    if (tid == 0) {
+      sv.k += 1;
+      bool refine = false;
+      if (sv.status == SPMV_SUCCESS) {
+        sv.rr_new = total;
+        sv.rr_max = fmax(sv.rr_max, total);
+        refine = total < sv.delta2 * sv.rr_max || total / sv.rr0 < sv.rtol2 ||
+                 sv.k >= sv.kmax || !isfinite(total);
+        sv.rr_prev = sv.rr;
+        sv.beta = total / sv.rr;
+        sv.rr = total;
+      }
+      sv.c = 0.0;
+      sv.refine = refine ? 1 : 0;
+    }
+    named_sync(1, NT);
+    if (sv.refine) {
+      // Fold (ir_fold): x += d + alpha p, d = 0.
+      for (int g = me.g0 + tid; g < me.g1; g += NT) {
+        const float di = c.d[g] + alpha32 * c.p[g];
+        c.x[g] = c.x[g] + double(di);
+        c.d[g] = 0.0f;
+      }
+      if (!barrier()) {
+        ok = false;
+        break;
+      }
+      // Residual and resync (ir_residual, ir_resync): r = fl32(b - A x).
+      double t3[3] = {0.0, 0.0, 0.0};
+      ir_fused_residual<CFG::NC, D16>(a64, c.tiles32, me.t0, me.t1, c.x, c.b,
+                                      [&](int g, double r64) {
+                                        const float ri = float(r64);
+                                        r_at(g) = ri;
+                                        t3[0] += r64 * r64;
+                                        t3[1] += double(ri) * double(ri);
+                                        t3[2] += double(ri) * double(c.p[g]);
+                                      });
+      double o3[3];
+      ++epoch;
+      if (!coop_grid_sum_n<NT, 3>(t3, parts(epoch), c.bar, epoch * gridDim.x, err, c.wait_ns,
+                                  gs3, o3)) {
+        ok = false;
+        break;
+      }
+      if (tid == 0) {
+        sv.rr_true = o3[0];
+        sv.refinements += 1;
+        sv.rr_max = o3[0];
+        if (o3[0] / sv.rr0 < sv.rtol2) sv.converged = 1;
+        if (!isfinite(o3[0])) sv.status = SPMV_ERROR_BREAKDOWN;
+        sv.beta = o3[1] / sv.rr_prev;
+        sv.rr = o3[1];
+        sv.c = o3[2] / o3[1];
+      }
+      named_sync(1, NT);
+    }
+    // C (ir_update_p): d += alpha p (unless folded), p = r + beta (p - c r).
+    const bool stop = sv.status != SPMV_SUCCESS || sv.converged;
+    if (!stop) {
+      const float beta32 = float(sv.beta);
+      const float cc = float(sv.c);
+      const bool fold_d = sv.refine == 0;
+      for (int g = me.g0 + tid; g < me.g1; g += NT) {
+        const float ri = r_at(g);
+        const float pi = ld_pol(c.p + g, keep);
+        if (fold_d) st_pol(c.d + g, ld_pol(c.d + g, keep) + alpha32 * pi, keep);
+        st_pol(c.p + g, ri + beta32 * (pi - cc * ri), keep);
+      }
+    }
+    if (tid == 0) {
+      sv.k_guard += 1;
+      sv.go = !stop && sv.k < sv.kmax && sv.k_guard < sv.kmax;
+    }
+    named_sync(1, NT);
+    if (!sv.go) break;
+    if (!barrier()) {  // A gathers p
+      ok = false;
+      break;
+    }
+  }
+  if (tid == 0) {
+    pipe.stop = 1;
+    if (ok && blockIdx.x == 0) {
+      IrState* st = c.st;
+      st->rr0 = sv.rr0;
+      st->rr = sv.rr;
+      st->rr_new = sv.rr_new;
+      st->rr_max = sv.rr_max;
+      st->alpha = sv.alpha;
+      st->beta = sv.beta;
+      st->pap = sv.pap;
+      st->c = sv.c;
+      st->rr_true = sv.rr_true;
+      st->rr_prev = sv.rr_prev;
+      st->k = sv.k;
+      st->status = sv.status;
+      st->converged = sv.converged;
+      st->refine = sv.refine;
+      st->refinements = sv.refinements;
+      st->k_guard = sv.k_guard;
+    }
+  }
+}
+
+using IrFusedFn = void (*)(SpmvArgs, SpmvArgs, IrPtrs, const FusedCta*);
+using IrFusedTwo = StagedCfg<12, 3, 16384, 2>;
+
+template <bool D16, bool RS>
+IrFusedFn ir_fused_fn_u(int U) {
+  switch (staged_width(U)) {
+    case 9: return ir_fused<IrFusedTwo, 9, D16, RS>;
+    case 8: return ir_fused<IrFusedTwo, 8, D16, RS>;
+    case 7: return ir_fused<IrFusedTwo, 7, D16, RS>;
+    case 5: return ir_fused<IrFusedTwo, 5, D16, RS>;
+    default: return ir_fused<IrFusedTwo, 4, D16, RS>;
+  }
+}
+IrFusedFn ir_fused_fn(const SolverProduct& p, bool rs) {
+  if (p.d16) return rs ? ir_fused_fn_u<true, true>(p.w) : ir_fused_fn_u<true, false>(p.w);
+  return rs ? ir_fused_fn_u<false, true>(p.w) : ir_fused_fn_u<false, false>(p.w);
+}
+
 __global__ void to_float(const double* __restrict__ in, float* __restrict__ out,
                          int64_t n) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
@@ -428,6 +793,8 @@ IrPtrs ir_ptrs(IrWorkspace& w) {
   c.tiles64 = w.tiles64;
   c.ntiles32 = w.ntiles32;
   c.ntiles64 = w.ntiles64;
+  c.bar = w.bar.as<unsigned long long>();
+  c.wait_ns = fused_wait_ns();
   return c;
 }
 
@@ -541,6 +908,154 @@ void build_ir_graph(spmv_matrix A, IrWorkspace& w) {
   SPMVB_CUDA(cudaGraphInstantiate(&w.exec, w.graph, 0));
 }
 
+// Fused plans: two CTAs per SM over the FP32 product's tiles, the CTA's rows
+// of r in shared memory (RS) or in global memory.
+template <bool RS>
+bool ir_plan(spmv_matrix A, const IrWorkspace& w, FusedPlan& plan) {
+  static_assert(IrFusedTwo::max_entries(6) == SolverStaged::max_entries(6) &&
+                    IrFusedTwo::max_entries(8) == SolverStaged::max_entries(8),
+                "the fused shape uses the solver product's tiles");
+  const int eb = entry_bytes(w.p32, true);
+  return fused_plan(A, ir_tiles(A, w.p32, true), (const void*)ir_fused_fn(w.p32, RS),
+                    IrFusedTwo::BS, IrFusedTwo::MINB, IrFusedTwo::smem_bytes(eb), RS ? 4 : 0,
+                    plan);
+}
+
+void ir_use_plan(IrWorkspace& w, const FusedPlan& plan) {
+  w.fused = true;
+  w.fused_fn = plan.fn;
+  w.fused_grid = plan.grid;
+  w.fused_block = plan.block;
+  w.fused_smem = plan.smem;
+  w.fused_rs = plan.rs;
+  w.fpartials.reserve(sizeof(double) * 6 * size_t(plan.grid));  // 2 arrays of 3 per CTA
+  w.ctas.reserve(sizeof(FusedCta) * plan.ctas.size());
+  SPMVB_CUDA(cudaMemcpy(w.ctas.ptr, plan.ctas.data(), sizeof(FusedCta) * plan.ctas.size(),
+                        cudaMemcpyHostToDevice));
+}
+
+// One solve as ir_run enqueues it: kmax, rtol^2, delta^2 and the error
+// flag, then the fused launch or the graph.
+void ir_enqueue(IrWorkspace& w, cudaStream_t s) {
+  IrState* st = w.state.as<IrState>();
+  SPMVB_CUDA(cudaMemcpyAsync(&st->kmax, &w.host.kmax, sizeof(int), cudaMemcpyHostToDevice, s));
+  SPMVB_CUDA(cudaMemcpyAsync(&st->rtol2, &w.host.rtol2, 2 * sizeof(double),
+                             cudaMemcpyHostToDevice, s));
+  if (w.fused) {
+    const size_t g = size_t(w.fused_grid);
+    require(w.fpartials.bytes >= 6 * g * sizeof(double) &&
+                w.ctas.bytes >= g * sizeof(FusedCta) && w.tiles32 != nullptr,
+            "spmv: fused mixed CG buffers smaller than its grid");
+    SPMVB_CUDA(cudaMemsetAsync(&st->stage_err, 0, sizeof(int), s));
+    SPMVB_CUDA(cudaMemsetAsync(w.bar.ptr, 0, sizeof(unsigned long long), s));
+    IrPtrs c = ir_ptrs(w);
+    c.partials = w.fpartials.as<double>();
+    const FusedCta* ctas = w.ctas.as<FusedCta>();
+    void* args[] = {&w.fa32, &w.fa64, &c, &ctas};
+    const cudaError_t e = cudaLaunchCooperativeKernel(
+        w.fused_fn, dim3(w.fused_grid), dim3(w.fused_block), args, size_t(w.fused_smem), s);
+    if (e != cudaErrorCooperativeLaunchTooLarge) {
+      SPMVB_CUDA(e);
+      return;
+    }
+    // The grid no longer fits on the device at once: this solve and the
+    // later ones run in the graph form (the refused launch ran nothing).
+    (void)cudaGetLastError();
+    w.fused = false;
+  }
+  SPMVB_CUDA(cudaGraphLaunch(w.exec, s));
+}
+
+__global__ void ir_fill(double* v, int64_t n, double value) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    v[i] = value;
+}
+
+// Device time of `its` inner iterations of the current form (b = 1, no
+// convergence test can pass; the refinements fall where they fall in
+// either form), best of three.
+float ir_time(IrWorkspace& w, cudaStream_t s, int its) {
+  w.host.kmax = its;
+  w.host.rtol2 = 0.0;
+  w.host.delta2 = 0.01;
+  cudaEvent_t e0, e1;
+  SPMVB_CUDA(cudaEventCreate(&e0));
+  SPMVB_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    SPMVB_CUDA(cudaEventRecord(e0, s));
+    ir_enqueue(w, s);
+    SPMVB_CUDA(cudaEventRecord(e1, s));
+    SPMVB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SPMVB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (rep > 0) best = std::min(best, ms);
+  }
+  SPMVB_CUDA(cudaEventDestroy(e0));
+  SPMVB_CUDA(cudaEventDestroy(e1));
+  SPMVB_CUDA(cudaMemcpy(&w.host, w.state.ptr, sizeof(IrState), cudaMemcpyDeviceToHost));
+  if (w.host.stage_err)
+    fail(SPMV_ERROR_CUDA, "spmv: a bounded wait of the fused mixed CG solve timed out");
+  return best;
+}
+
+// Chooses between the graph form and the fused plans that fit (the FP32
+// product must be staged), by timing a few inner iterations of each.
+// SPMV_B200_CG_MIXED_FUSED: "0" keeps the graph form; "smem" or "global"
+// forces that plan, failing if it does not fit.
+void ir_choose_form(spmv_matrix A, IrWorkspace& w) {
+  w.fused = false;
+  if (w.p32.kind != ProductKind::Staged || w.n == 0) return;
+  const char* env = std::getenv("SPMV_B200_CG_MIXED_FUSED");
+  const std::string mode = env ? env : "";
+  if (mode == "0") return;
+  spmv_comm comm = A->comm;
+  int coop = 0;
+  SPMVB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, comm->device));
+  if (!coop) return;
+  if (!ir_tiles(A, w.p32, true).ok) return;
+  w.bar.reserve(sizeof(unsigned long long));
+  ir_args(A, w, w.p32, true, w.fa32);
+  SolverProduct s64 = w.p32;  // the FP64 residual walks the same SELL slices
+  ir_args(A, w, s64, false, w.fa64);
+  if (!mode.empty()) {
+    FusedPlan p;
+    bool fits = false;
+    if (mode == "smem") fits = ir_plan<true>(A, w, p);
+    else if (mode == "global") fits = ir_plan<false>(A, w, p);
+    require(fits, "spmv: SPMV_B200_CG_MIXED_FUSED must be 0 or a fused plan that fits this "
+                  "matrix (smem, global)");
+    ir_use_plan(w, p);
+    return;
+  }
+  std::vector<FusedPlan> plans;
+  {
+    FusedPlan p1, p2;
+    if (ir_plan<true>(A, w, p1)) plans.push_back(std::move(p1));
+    if (ir_plan<false>(A, w, p2)) plans.push_back(std::move(p2));
+  }
+  if (plans.empty()) return;
+  cudaStream_t s = comm->stream;
+  const int its = 16;
+  SPMVB_CUDA(cudaDeviceSynchronize());
+  ir_fill<<<std::max(1, comm->num_sms) * 4, 256, 0, s>>>(w.b.as<double>(), w.n, 1.0);
+  SPMVB_CUDA(cudaGetLastError());
+  float best = ir_time(w, s, its);
+  int pick = -1;
+  for (size_t i = 0; i < plans.size(); ++i) {
+    ir_use_plan(w, plans[i]);
+    const float t = ir_time(w, s, its);
+    if (!w.fused) continue;  // the plan's launch was refused (graph form ran)
+    if (t < best) {
+      best = t;
+      pick = int(i);
+    }
+  }
+  w.fused = false;
+  if (pick >= 0) ir_use_plan(w, plans[size_t(pick)]);
+}
+
 }  // namespace
 
 void destroy_ir_workspace(IrWorkspace* w) { delete w; }
@@ -617,9 +1132,20 @@ IrWorkspace& ir_workspace(spmv_matrix A) {
     use_tiles(ws.p32, true);
     use_tiles(ws.p64, false);
     build_ir_graph(A, *w);
+    ir_choose_form(A, *w);
     A->ir = std::move(w);
   }
   return *A->ir;
+}
+
+CgForm ir_form(spmv_matrix A) {
+  require(A->ir != nullptr, "spmv: spmv_cg_mixed has not run on this matrix");
+  const IrWorkspace& w = *A->ir;
+  CgForm f;
+  f.fused = w.fused;
+  f.cps = w.fused ? IrFusedTwo::MINB : 0;
+  f.rs = w.fused && w.fused_rs;
+  return f;
 }
 
 SolverProduct ir_product(spmv_matrix A, bool fp32) {
@@ -637,15 +1163,11 @@ void ir_run(spmv_matrix A, int max_its, double rtol, spmv_ir_info* info) {
   w.host.kmax = max_its;
   w.host.rtol2 = rtol * rtol;
   w.host.delta2 = 0.01;  // refine when ||r|| fell 10x below its recent maximum
-  SPMVB_CUDA(cudaMemcpyAsync(&st->kmax, &w.host.kmax, sizeof(int),
-                             cudaMemcpyHostToDevice, s));
-  SPMVB_CUDA(cudaMemcpyAsync(&st->rtol2, &w.host.rtol2, 2 * sizeof(double),
-                             cudaMemcpyHostToDevice, s));
-  SPMVB_CUDA(cudaGraphLaunch(w.exec, s));
+  ir_enqueue(w, s);
   SPMVB_CUDA(cudaMemcpyAsync(&w.host, st, sizeof(IrState), cudaMemcpyDeviceToHost, s));
   SPMVB_CUDA(cudaStreamSynchronize(s));
   if (w.host.stage_err)
-    fail(SPMV_ERROR_CUDA, "spmv: a staged product's bounded wait timed out");
+    fail(SPMV_ERROR_CUDA, "spmv: a bounded wait on the device timed out");
   if (info) {
     info->iterations = w.host.k;
     info->refinements = w.host.refinements;

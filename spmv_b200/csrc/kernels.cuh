@@ -391,4 +391,63 @@ __device__ __forceinline__ bool coop_grid_sum(double v, double* parts, unsigned 
   return true;
 }
 
+// N sums at once, the same way: parts holds N partials per CTA (CTA b's at
+// parts[N b .. N b + N - 1]); every CTA gets the same N totals.
+template <int NT, int N>
+struct GridSumN {
+  double red[N][NT / 32];
+  double total[N];
+  int ok;
+};
+
+template <int NT, int N>
+__device__ __forceinline__ bool coop_grid_sum_n(const double (&v)[N], double* parts,
+                                                unsigned long long* count,
+                                                unsigned long long target, int* err,
+                                                unsigned long long limit_ns, GridSumN<NT, N>& s,
+                                                double (&total)[N]) {
+  const int warp = int(threadIdx.x) >> 5, lane = int(threadIdx.x) & 31;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    double x = v[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) s.red[j][warp] = x;
+  }
+  named_sync(1, NT);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      double t = 0.0;
+      for (int w = 0; w < NT / 32; ++w) t += s.red[j][w];
+      __stcg(parts + N * blockIdx.x + j, t);
+    }
+    s.ok = grid_arrive_wait(count, target, err, limit_ns);
+  }
+  named_sync(1, NT);
+  if (!s.ok) return false;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    double t = 0.0;
+    for (unsigned int i = threadIdx.x; i < gridDim.x; i += unsigned(NT))
+      t += __ldcg(parts + N * i + j);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) s.red[j][warp] = t;
+  }
+  named_sync(1, NT);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      double t = 0.0;
+      for (int w = 0; w < NT / 32; ++w) t += s.red[j][w];
+      s.total[j] = t;
+    }
+  }
+  named_sync(1, NT);
+#pragma unroll
+  for (int j = 0; j < N; ++j) total[j] = s.total[j];
+  return true;
+}
+
 }  // namespace spmvb
