@@ -203,7 +203,8 @@ def _timed(stream, fn, reps):
 
 def run_extras(device: int, reps: int, c4_count: int):
     """c3: 27-point lognormal Laplacian 160^3 (4,096,000 rows), FP64 CG vs
-    mixed CG, both to ||b - A x|| / ||b|| < 1e-10.  c4: `c4_count` k-NN
+    mixed CG, both to ||b - A x|| / ||b|| < 1e-10; the same on the 7-point
+    128^3 Poisson matrix over 8 ranks (the CG workload).  c4: `c4_count` k-NN
     systems of 4,096..131,072 rows, one batched persistent launch vs one
     plain FP64 CG solve per system.  c5: one adjoint (forward solve, adjoint
     solve, dL/dA sampling) on the 1024^2 grid."""
@@ -241,8 +242,39 @@ def run_extras(device: int, reps: int, c4_count: int):
         "error_mixed_vs_fp64_solution": err, "mult_kernel": tune[:3],
         "cg_product": M.solver_product("cg"),
         "mixed_products": [M.solver_product("mixed32"), M.solver_product("mixed64")],
+        "cg_form": M.cg_form(), "mixed_form": M.cg_form("mixed"),
         "setup_s": setup_s}
     del M, cm, b, x64, xm
+    torch.cuda.empty_cache()
+    # c2 mixed ----------------------------------------------------------------
+    W = gen.workload("c2")
+    D = gen.distribute(W.A, W.P)
+    comm2 = S.Comm(size=W.P, device=device)
+    stream2 = comm2.torch_stream()
+    cm = S.L2GMap(comm2, D.local_sizes, D.ghosts)
+    rm = S.L2GMap(comm2, D.local_sizes, [[] for _ in range(W.P)])
+    M = S.Matrix(comm2, D.blocks, cm, rm)
+    b = [torch.from_numpy(W.b[D.ranges[q]:D.ranges[q + 1]].copy()).cuda(device)
+         for q in range(W.P)]
+    x64 = [torch.zeros(cm.vec_len(q), dtype=torch.float64, device=f"cuda:{device}")
+           for q in range(W.P)]
+    xm = [torch.zeros_like(v) for v in x64]
+    S.cg(comm2, M, b, 20000, 1e-10, x=x64)
+    S.cg_mixed(comm2, M, b, 20000, 1e-10, x=xm)
+    t64, (_, k64) = _timed(stream2, lambda: S.cg(comm2, M, b, 20000, 1e-10, x=x64), reps)
+    tmx, (_, im) = _timed(stream2, lambda: S.cg_mixed(comm2, M, b, 20000, 1e-10, x=xm), reps)
+    xa = torch.cat([xm[q][:D.local_sizes[q]] for q in range(W.P)])
+    xb = torch.cat([x64[q][:D.local_sizes[q]] for q in range(W.P)])
+    out["c2_mixed_vs_fp64"] = {
+        "fp64_cg_solves_per_s": 1.0 / t64, "fp64_iterations": k64,
+        "mixed_solves_per_s": 1.0 / tmx, "mixed_inner_iterations": im.iterations,
+        "mixed_refinements": im.refinements, "speedup": t64 / tmx,
+        "relres_mixed": im.relres,
+        "error_mixed_vs_fp64_solution": float(torch.linalg.norm(xa - xb) /
+                                              torch.linalg.norm(xb)),
+        "cg_form": M.cg_form(), "mixed_form": M.cg_form("mixed"),
+        "mixed_products": [M.solver_product("mixed32"), M.solver_product("mixed64")]}
+    del M, cm, rm, b, x64, xm
     torch.cuda.empty_cache()
     # c4 ----------------------------------------------------------------------
     t0 = time.perf_counter()
