@@ -53,7 +53,7 @@ struct IrWorkspace {
   // Fused form (one cooperative launch per solve), when chosen.
   bool fused = false;
   const void* fused_fn = nullptr;
-  int fused_grid = 0, fused_block = 0, fused_smem = 0;
+  int fused_grid = 0, fused_block = 0, fused_smem = 0, fused_cps = 0;
   bool fused_rs = false;
   spmvb::DevBuf bar, fpartials, ctas;
   spmvb::SpmvArgs fa32, fa64;  // FP32 product over p, FP64 SELL over x
@@ -367,13 +367,12 @@ __device__ __forceinline__ double ir_fused_product(const SpmvArgs& a, int count,
 // The refinement's FP64 residual over the CTA's slices (tiles t0..t1 of
 // the FP32 table: the same slices in the FP64 SELL arrays), one warp per
 // slice, each row summed in storage order; f(g, r64) per row.
-template <int NW, bool D16, class F>
+template <int NW, int U, bool D16, class F>
 __device__ __forceinline__ void ir_fused_residual(const SpmvArgs& a,
                                                   const StagedDesc* __restrict__ tiles, int t0,
                                                   int t1, const double* __restrict__ x,
                                                   const double* __restrict__ b, F&& f) {
   using CI = typename std::conditional<D16, int16_t, int32_t>::type;
-  constexpr int U = 4;
   const int warp = int(threadIdx.x) >> 5, lane = int(threadIdx.x) & 31;
   int q = warp;
   for (int t = t0; t < t1; ++t) {
@@ -424,7 +423,11 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
   using CI = typename std::conditional<D16, int16_t, int32_t>::type;
   constexpr int NT = CFG::NC * 32;
   constexpr int STAGES_BYTES = CFG::smem_bytes(4 + int(sizeof(CI)));
-  constexpr int V = 4;
+  // Rows per thread in flight in the vector phase and entries per lane in
+  // flight in the refinement's residual: as many as the shape's registers
+  // hold without spilling.
+  constexpr int V = CFG::MINB == 3 ? 1 : 4;
+  constexpr int UR = CFG::MINB == 3 ? 2 : 4;
   extern __shared__ __align__(128) unsigned char staged_smem[];
   __shared__ StagedLoop<CFG> pipe;
   __shared__ GridSumN<NT, 1> gs1;
@@ -583,7 +586,7 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
       }
       // Residual and resync (ir_residual, ir_resync): r = fl32(b - A x).
       double t3[3] = {0.0, 0.0, 0.0};
-      ir_fused_residual<CFG::NC, D16>(a64, c.tiles32, me.t0, me.t1, c.x, c.b,
+      ir_fused_residual<CFG::NC, UR, D16>(a64, c.tiles32, me.t0, me.t1, c.x, c.b,
                                       [&](int g, double r64) {
                                         const float ri = float(r64);
                                         r_at(g) = ri;
@@ -660,20 +663,21 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
 
 using IrFusedFn = void (*)(SpmvArgs, SpmvArgs, IrPtrs, const FusedCta*);
 using IrFusedTwo = StagedCfg<12, 3, 16384, 2>;
+using IrFusedThree = StagedCfg<12, 4, 16384, 3>;
 
-template <bool D16, bool RS>
+template <class CFG, bool D16, bool RS>
 IrFusedFn ir_fused_fn_u(int U) {
   switch (staged_width(U)) {
-    case 9: return ir_fused<IrFusedTwo, 9, D16, RS>;
-    case 8: return ir_fused<IrFusedTwo, 8, D16, RS>;
-    case 7: return ir_fused<IrFusedTwo, 7, D16, RS>;
-    case 5: return ir_fused<IrFusedTwo, 5, D16, RS>;
-    default: return ir_fused<IrFusedTwo, 4, D16, RS>;
+    case 9: return ir_fused<CFG, 9, D16, RS>;
+    case 8: return ir_fused<CFG, 8, D16, RS>;
+    case 7: return ir_fused<CFG, 7, D16, RS>;
+    case 5: return ir_fused<CFG, 5, D16, RS>;
+    default: return ir_fused<CFG, 4, D16, RS>;
   }
 }
-IrFusedFn ir_fused_fn(const SolverProduct& p, bool rs) {
-  if (p.d16) return rs ? ir_fused_fn_u<true, true>(p.w) : ir_fused_fn_u<true, false>(p.w);
-  return rs ? ir_fused_fn_u<false, true>(p.w) : ir_fused_fn_u<false, false>(p.w);
+template <class CFG, bool RS>
+IrFusedFn ir_fused_fn(const SolverProduct& p) {
+  return p.d16 ? ir_fused_fn_u<CFG, true, RS>(p.w) : ir_fused_fn_u<CFG, false, RS>(p.w);
 }
 
 __global__ void to_float(const double* __restrict__ in, float* __restrict__ out,
@@ -908,17 +912,16 @@ void build_ir_graph(spmv_matrix A, IrWorkspace& w) {
   SPMVB_CUDA(cudaGraphInstantiate(&w.exec, w.graph, 0));
 }
 
-// Fused plans: two CTAs per SM over the FP32 product's tiles, the CTA's rows
-// of r in shared memory (RS) or in global memory.
-template <bool RS>
+// Fused plans over the FP32 product's tiles: shape CFG (CFG::MINB CTAs per
+// SM), the CTA's rows of r in shared memory (RS) or in global memory.
+template <class CFG, bool RS>
 bool ir_plan(spmv_matrix A, const IrWorkspace& w, FusedPlan& plan) {
-  static_assert(IrFusedTwo::max_entries(6) == SolverStaged::max_entries(6) &&
-                    IrFusedTwo::max_entries(8) == SolverStaged::max_entries(8),
+  static_assert(CFG::max_entries(6) == SolverStaged::max_entries(6) &&
+                    CFG::max_entries(8) == SolverStaged::max_entries(8),
                 "the fused shape uses the solver product's tiles");
   const int eb = entry_bytes(w.p32, true);
-  return fused_plan(A, ir_tiles(A, w.p32, true), (const void*)ir_fused_fn(w.p32, RS),
-                    IrFusedTwo::BS, IrFusedTwo::MINB, IrFusedTwo::smem_bytes(eb), RS ? 4 : 0,
-                    plan);
+  return fused_plan(A, ir_tiles(A, w.p32, true), (const void*)ir_fused_fn<CFG, RS>(w.p32),
+                    CFG::BS, CFG::MINB, CFG::smem_bytes(eb), RS ? 4 : 0, plan);
 }
 
 void ir_use_plan(IrWorkspace& w, const FusedPlan& plan) {
@@ -927,6 +930,7 @@ void ir_use_plan(IrWorkspace& w, const FusedPlan& plan) {
   w.fused_grid = plan.grid;
   w.fused_block = plan.block;
   w.fused_smem = plan.smem;
+  w.fused_cps = plan.cps;
   w.fused_rs = plan.rs;
   w.fpartials.reserve(sizeof(double) * 6 * size_t(plan.grid));  // 2 arrays of 3 per CTA
   w.ctas.reserve(sizeof(FusedCta) * plan.ctas.size());
@@ -1001,9 +1005,13 @@ float ir_time(IrWorkspace& w, cudaStream_t s, int its) {
 }
 
 // Chooses between the graph form and the fused plans that fit (the FP32
-// product must be staged), by timing a few inner iterations of each.
-// SPMV_B200_CG_MIXED_FUSED: "0" keeps the graph form; "smem" or "global"
-// forces that plan, failing if it does not fit.
+// product must be staged), by the device time of inner iterations 9..40 of
+// each (a 40-iteration solve less an 8-iteration one: both end in the
+// refinement the iteration cap forces, which cancels): two
+// CTAs per SM of 3 stages with r in shared or global memory, or three of 4
+// stages (the graph form's product shape) with r in global memory.
+// SPMV_B200_CG_MIXED_FUSED: "0" keeps the graph form; "2:smem", "2:global"
+// or "3:global" forces that plan, failing if it does not fit.
 void ir_choose_form(spmv_matrix A, IrWorkspace& w) {
   w.fused = false;
   if (w.p32.kind != ProductKind::Staged || w.n == 0) return;
@@ -1022,30 +1030,32 @@ void ir_choose_form(spmv_matrix A, IrWorkspace& w) {
   if (!mode.empty()) {
     FusedPlan p;
     bool fits = false;
-    if (mode == "smem") fits = ir_plan<true>(A, w, p);
-    else if (mode == "global") fits = ir_plan<false>(A, w, p);
+    if (mode == "2:smem") fits = ir_plan<IrFusedTwo, true>(A, w, p);
+    else if (mode == "2:global") fits = ir_plan<IrFusedTwo, false>(A, w, p);
+    else if (mode == "3:global") fits = ir_plan<IrFusedThree, false>(A, w, p);
     require(fits, "spmv: SPMV_B200_CG_MIXED_FUSED must be 0 or a fused plan that fits this "
-                  "matrix (smem, global)");
+                  "matrix (2:smem, 2:global, 3:global)");
     ir_use_plan(w, p);
     return;
   }
   std::vector<FusedPlan> plans;
   {
-    FusedPlan p1, p2;
-    if (ir_plan<true>(A, w, p1)) plans.push_back(std::move(p1));
-    if (ir_plan<false>(A, w, p2)) plans.push_back(std::move(p2));
+    FusedPlan p1, p2, p3;
+    if (ir_plan<IrFusedTwo, true>(A, w, p1)) plans.push_back(std::move(p1));
+    if (ir_plan<IrFusedTwo, false>(A, w, p2)) plans.push_back(std::move(p2));
+    if (ir_plan<IrFusedThree, false>(A, w, p3)) plans.push_back(std::move(p3));
   }
   if (plans.empty()) return;
   cudaStream_t s = comm->stream;
-  const int its = 16;
   SPMVB_CUDA(cudaDeviceSynchronize());
   ir_fill<<<std::max(1, comm->num_sms) * 4, 256, 0, s>>>(w.b.as<double>(), w.n, 1.0);
   SPMVB_CUDA(cudaGetLastError());
-  float best = ir_time(w, s, its);
+  auto slope = [&]() { return ir_time(w, s, 40) - ir_time(w, s, 8); };
+  float best = slope();
   int pick = -1;
   for (size_t i = 0; i < plans.size(); ++i) {
     ir_use_plan(w, plans[i]);
-    const float t = ir_time(w, s, its);
+    const float t = slope();
     if (!w.fused) continue;  // the plan's launch was refused (graph form ran)
     if (t < best) {
       best = t;
@@ -1143,7 +1153,7 @@ CgForm ir_form(spmv_matrix A) {
   const IrWorkspace& w = *A->ir;
   CgForm f;
   f.fused = w.fused;
-  f.cps = w.fused ? IrFusedTwo::MINB : 0;
+  f.cps = w.fused ? w.fused_cps : 0;
   f.rs = w.fused && w.fused_rs;
   return f;
 }

@@ -1,13 +1,15 @@
 """Runs the kernels of one workload a few times, for profilers (ncu).
 
-    python -m spmv_b200.profile_case --case c2 --reps 3 [--what matvec|cg]
+    python -m spmv_b200.profile_case --case c2 --reps 3 [--what matvec|cg|mixed]
         [--kernel staged --width 7] [--cg-form 0|2:smem|...]
 
 `matvec` runs the reference matvec demo's loop body (matvecmain.cpp:70-86):
 L2GMap::update then Matrix::mult over all ranks, `reps` times, as plain
 kernel launches.  `cg` runs one spmv::cg solve: a CUDA graph, or one
 cooperative launch of the fused kernel (`--cg-form` forces the form through
-SPMV_B200_CG_FUSED, so no timing launches precede the solve).
+SPMV_B200_CG_FUSED, so no timing launches precede the solve).  `mixed`
+runs one mixed-precision solve to 1e-10 (`--cg-form` then forces its form
+through SPMV_B200_CG_MIXED_FUSED).
 """
 from __future__ import annotations
 
@@ -21,7 +23,7 @@ def main():
     ap.add_argument("--case", default="c2")
     ap.add_argument("--scale", type=int, default=0)
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--what", default="matvec", choices=["matvec", "cg"])
+    ap.add_argument("--what", default="matvec", choices=["matvec", "cg", "mixed"])
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--kernel", default="auto", choices=["auto", "vector", "merge", "sell", "staged"])
     ap.add_argument("--width", type=int, default=0)
@@ -29,7 +31,8 @@ def main():
     args = ap.parse_args()
     if args.cg_form is not None:
         import os
-        os.environ["SPMV_B200_CG_FUSED"] = args.cg_form
+        var = "SPMV_B200_CG_MIXED_FUSED" if args.what == "mixed" else "SPMV_B200_CG_FUSED"
+        os.environ[var] = args.cg_form
 
     import torch
     import spmv_b200 as S
@@ -52,6 +55,13 @@ def main():
             M.mult(xs, out=ys)
         comm.synchronize()
         print("matvec", args.case, "reps", args.reps, "kernel", M.get_kernel())
+    elif args.what == "mixed":
+        b = [torch.from_numpy(W.b[D.ranges[q]:D.ranges[q + 1]].copy()).cuda()
+             for q in range(W.P)]
+        x, info = S.cg_mixed(comm, M, b, 20000, 1e-10)
+        print("mixed", args.case, "inner iterations", info.iterations, "refinements",
+              info.refinements, "form", M.cg_form("mixed"), "products",
+              M.solver_product("mixed32"), M.solver_product("mixed64"))
     else:
         b = [torch.from_numpy(W.b[D.ranges[q]:D.ranges[q + 1]].copy()).cuda()
              for q in range(W.P)]

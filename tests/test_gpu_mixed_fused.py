@@ -1,10 +1,11 @@
 """The fused mixed-precision CG solve (FP32 inner iterations with FP64
 refinement as one cooperative launch of persistent CTAs) against its graph
 form (three kernels per inner iteration, three more per refinement) on the
-same matrix and staged products, for both fused plans: the FP32 residual in
-shared or global memory.  Also the edge cases through the fused form: zero
-right-hand side, the iteration cap, ranks with no rows, run-to-run
-reproducibility and a grid wait that runs out."""
+same matrix and staged products, for every fused plan: two CTAs per SM with
+the FP32 residual in shared or global memory, or three with it in global
+memory.  Also the edge cases through the fused form: zero right-hand side,
+the iteration cap, ranks with no rows, run-to-run reproducibility and a grid
+wait that runs out."""
 import numpy as np
 import pytest
 
@@ -14,7 +15,7 @@ from helpers import build
 
 pytestmark = pytest.mark.gpu
 
-PLANS = ["smem", "global"]
+PLANS = ["2:smem", "2:global", "3:global"]
 
 
 def solve(monkeypatch, plan, W, P, width, max_its=20000, rtol=1e-10):
@@ -47,7 +48,8 @@ def test_mixed_fused_matches_graph_form(monkeypatch, cuda_device, plan, cfg, sca
     x0, i0, M0, _, _ = solve(monkeypatch, "0", W, P, width)
     assert M0.cg_form("mixed") == ("graph", 0, None)
     x1, i1, M1, _, _ = solve(monkeypatch, plan, W, P, width)
-    assert M1.cg_form("mixed") == ("fused", 2, plan)
+    cps, where = plan.split(":")
+    assert M1.cg_form("mixed") == ("fused", int(cps), where)
     assert M1.solver_product("mixed32")[0] == "staged"
     assert i0.status == 0 and i1.status == 0
     assert i0.converged == 1 and i1.converged == 1
@@ -106,7 +108,7 @@ def test_mixed_fused_wait_limit(monkeypatch, cuda_device):
     CTA leaves, and the host reports the timeout.  The context stays usable:
     the same matrix then solves with the default bound."""
     W = gen.workload("c2", 32)
-    monkeypatch.setenv("SPMV_B200_CG_MIXED_FUSED", "smem")
+    monkeypatch.setenv("SPMV_B200_CG_MIXED_FUSED", "2:smem")
     comm, cm, rm, M, D = build(W, 8)
     M.set_kernel("staged", 7)
     b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(8)]
