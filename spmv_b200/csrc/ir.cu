@@ -976,13 +976,13 @@ __global__ void ir_fill(double* v, int64_t n, double value) {
     v[i] = value;
 }
 
-// Device time of `its` inner iterations of the current form (b = 1, no
-// convergence test can pass; the refinements fall where they fall in
-// either form), best of three.
+// Device time of a solve of `its` inner iterations in the current form
+// (b = 1, no convergence test can pass, delta2 = 0: no refinement but the
+// one the iteration cap forces), best of three.
 float ir_time(IrWorkspace& w, cudaStream_t s, int its) {
   w.host.kmax = its;
   w.host.rtol2 = 0.0;
-  w.host.delta2 = 0.01;
+  w.host.delta2 = 0.0;
   cudaEvent_t e0, e1;
   SPMVB_CUDA(cudaEventCreate(&e0));
   SPMVB_CUDA(cudaEventCreate(&e1));
@@ -1005,9 +1005,11 @@ float ir_time(IrWorkspace& w, cudaStream_t s, int its) {
 }
 
 // Chooses between the graph form and the fused plans that fit (the FP32
-// product must be staged), by the device time of inner iterations 9..40 of
-// each (a 40-iteration solve less an 8-iteration one: both end in the
-// refinement the iteration cap forces, which cancels): two
+// product must be staged) by timing each: s = device time per inner
+// iteration (a 40-iteration solve less an 8-iteration one, over 32) and
+// F = the rest of the 8-iteration solve (launch, init and the refinement the
+// cap forces), scored s + F / 100: solves to 1e-10 refine about once per
+// 50..250 inner iterations.  The candidates are two
 // CTAs per SM of 3 stages with r in shared or global memory, or three of 4
 // stages (the graph form's product shape) with r in global memory.
 // SPMV_B200_CG_MIXED_FUSED: "0" keeps the graph form; "2:smem", "2:global"
@@ -1050,12 +1052,21 @@ void ir_choose_form(spmv_matrix A, IrWorkspace& w) {
   SPMVB_CUDA(cudaDeviceSynchronize());
   ir_fill<<<std::max(1, comm->num_sms) * 4, 256, 0, s>>>(w.b.as<double>(), w.n, 1.0);
   SPMVB_CUDA(cudaGetLastError());
-  auto slope = [&]() { return ir_time(w, s, 40) - ir_time(w, s, 8); };
-  float best = slope();
+  auto score = [&](const char* name) {
+    const float t8 = ir_time(w, s, 8), t40 = ir_time(w, s, 40);
+    const float per_it = (t40 - t8) / 32.f, fixed = t8 - 8.f * per_it;
+    debug_log(std::string("cg_mixed form ") + name + ": " + std::to_string(per_it * 1e3f) +
+              " us per inner iteration, " + std::to_string(fixed * 1e3f) +
+              " us per solve + refinement");
+    return per_it + fixed / 100.f;
+  };
+  float best = score("graph");
   int pick = -1;
   for (size_t i = 0; i < plans.size(); ++i) {
     ir_use_plan(w, plans[i]);
-    const float t = slope();
+    const std::string name = "fused " + std::to_string(plans[i].cps) +
+                             (plans[i].rs ? ":smem" : ":global");
+    const float t = score(name.c_str());
     if (!w.fused) continue;  // the plan's launch was refused (graph form ran)
     if (t < best) {
       best = t;
