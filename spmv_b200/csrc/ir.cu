@@ -366,7 +366,8 @@ __device__ __forceinline__ double ir_fused_product(const SpmvArgs& a, int count,
 
 // The refinement's FP64 residual over the CTA's slices (tiles t0..t1 of
 // the FP32 table: the same slices in the FP64 SELL arrays), one warp per
-// slice, each row summed in storage order; f(g, r64) per row.
+// slice, each row summed in storage order; f(g, r64, exists) by every lane
+// of the warp for each slice (exists: the lane's row is a row of the rank).
 template <int NW, int U, bool D16, class F>
 __device__ __forceinline__ void ir_fused_residual(const SpmvArgs& a,
                                                   const StagedDesc* __restrict__ tiles, int t0,
@@ -410,7 +411,8 @@ __device__ __forceinline__ void ir_fused_residual(const SpmvArgs& a,
         for (int u = 0; u < U; ++u)
           if (ok[u]) sum += v[u] * xv[u];
       }
-      if (row < P.nrows) f(g, b[g] - sum);
+      const bool exists = row < P.nrows;
+      f(g, exists ? b[g] - sum : 0.0, exists);
     }
     q -= ns;
   }
@@ -427,13 +429,14 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
   // flight in the refinement's residual: as many as the shape's registers
   // hold without spilling.
   constexpr int V = CFG::MINB == 3 ? 1 : 4;
-  constexpr int UR = CFG::MINB == 3 ? 2 : 4;
+  constexpr int UR = CFG::MINB == 3 ? 4 : 6;
   extern __shared__ __align__(128) unsigned char staged_smem[];
   __shared__ StagedLoop<CFG> pipe;
   __shared__ GridSumN<NT, 1> gs1;
   __shared__ GridSumN<NT, 2> gs2;
   __shared__ GridSumN<NT, 3> gs3;
   __shared__ GridSum<NT> gsb;
+  __shared__ double racc[CFG::NC][3];
   __shared__ FusedCta me;
   __shared__ IrScalars sv;
 
@@ -585,15 +588,41 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
         break;
       }
       // Residual and resync (ir_residual, ir_resync): r = fl32(b - A x).
+      // ||b - A x||^2, r.r and r.p: summed per slice across the warp and
+      // kept per warp in shared memory (no accumulators live across the
+      // gathers), then handed to the grid sum by each warp's lane 0.
+      const int warp = tid >> 5, lane = tid & 31;
+      if (lane == 0) racc[warp][0] = racc[warp][1] = racc[warp][2] = 0.0;
+      __syncwarp();
+      ir_fused_residual<CFG::NC, UR, D16>(
+          a64, c.tiles32, me.t0, me.t1, c.x, c.b, [&](int g, double r64, bool exists) {
+            const float ri = float(r64);
+            double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+            if (exists) {
+              r_at(g) = ri;
+              v0 = r64 * r64;
+              v1 = double(ri) * double(ri);
+              v2 = double(ri) * double(c.p[g]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+              v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+              v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+              v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+            }
+            if (lane == 0) {
+              racc[warp][0] += v0;
+              racc[warp][1] += v1;
+              racc[warp][2] += v2;
+            }
+          });
+      __syncwarp();
       double t3[3] = {0.0, 0.0, 0.0};
-      ir_fused_residual<CFG::NC, UR, D16>(a64, c.tiles32, me.t0, me.t1, c.x, c.b,
-                                      [&](int g, double r64) {
-                                        const float ri = float(r64);
-                                        r_at(g) = ri;
-                                        t3[0] += r64 * r64;
-                                        t3[1] += double(ri) * double(ri);
-                                        t3[2] += double(ri) * double(c.p[g]);
-                                      });
+      if (lane == 0) {
+        t3[0] = racc[warp][0];
+        t3[1] = racc[warp][1];
+        t3[2] = racc[warp][2];
+      }
       double o3[3];
       ++epoch;
       if (!coop_grid_sum_n<NT, 3>(t3, parts(epoch), c.bar, epoch * gridDim.x, err, c.wait_ns,
