@@ -96,7 +96,7 @@ def adjoint_grad(P: GridProblem, rtol):
     x = spd_solve(P.vals_torch(th), b, sysm)
     L = 0.5 * ((x - xs) ** 2).sum()
     L.backward()
-    return th.grad.cpu().numpy(), b.grad.cpu().numpy(), float(L), sysm
+    return th.grad.cpu().numpy(), b.grad.cpu().numpy(), float(L.detach()), sysm
 
 
 def test_adjoint_small_grid_against_direct_fp64(cuda_device):
