@@ -648,11 +648,26 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
       const float beta32 = float(sv.beta);
       const float cc = float(sv.c);
       const bool fold_d = sv.refine == 0;
-      for (int g = me.g0 + tid; g < me.g1; g += NT) {
-        const float ri = r_at(g);
-        const float pi = ld_pol(c.p + g, keep);
-        if (fold_d) st_pol(c.d + g, ld_pol(c.d + g, keep) + alpha32 * pi, keep);
-        st_pol(c.p + g, ri + beta32 * (pi - cc * ri), keep);
+      const int g1 = me.g1;
+      for (int g0 = me.g0 + tid; g0 < g1; g0 += V * NT) {
+        float pv[V], dv[V];
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+          const int g = g0 + u * NT;
+          if (g < g1) {
+            pv[u] = ld_pol(c.p + g, keep);
+            dv[u] = fold_d ? ld_pol(c.d + g, keep) : 0.0f;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+          const int g = g0 + u * NT;
+          if (g < g1) {
+            const float ri = r_at(g);
+            if (fold_d) st_pol(c.d + g, dv[u] + alpha32 * pv[u], keep);
+            st_pol(c.p + g, ri + beta32 * (pv[u] - cc * ri), keep);
+          }
+        }
       }
     }
     if (tid == 0) {
