@@ -425,9 +425,9 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
   using CI = typename std::conditional<D16, int16_t, int32_t>::type;
   constexpr int NT = CFG::NC * 32;
   constexpr int STAGES_BYTES = CFG::smem_bytes(4 + int(sizeof(CI)));
-  // Rows per thread in flight in the vector phase and entries per lane in
-  // flight in the refinement's residual: as many as the shape's registers
-  // hold without spilling.
+  // Rows per thread in flight in the vector phases (B and C) and entries
+  // per lane in flight in the refinement's residual: as many as the shape's
+  // registers hold without spilling.
   constexpr int V = CFG::MINB == 3 ? 1 : 4;
   constexpr int UR = CFG::MINB == 3 ? 4 : 6;
   extern __shared__ __align__(128) unsigned char staged_smem[];
