@@ -235,7 +235,9 @@ int spmv_matrix_set_values(spmv_matrix A, spmv_memory memory,
  *  - Limit: rows + nonzeros over all ranks of at most 33,554,432 (16384 tiles
  *    of 2048); a larger matrix is rejected with SPMV_ERROR_INVALID_ARGUMENT.
  *  - The first call on a device looks up the array's device address, once per
- *    device; make that first call before any stream capture.
+ *    device; make that first call before any stream capture.  The address is
+ *    kept for the life of the process: after cudaDeviceReset (which also ends
+ *    every handle of this library on that device) do not call it again.
  *  - All calls share the one array, which keeps what the last call left in it
  *    (each call writes every slot before reading it, so nothing needs
  *    clearing); calls that overlap on the GPU, e.g. from two streams of the

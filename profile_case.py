@@ -1,6 +1,6 @@
 """Runs the kernels of one workload a few times, for profilers (ncu).
 
-    python -m spmv_b200.profile_case --case c2 --reps 3 [--what matvec|cg|mixed]
+    python profile_case.py --case c2 --reps 3 [--what matvec|cg|mixed]
         [--kernel staged --width 7] [--cg-form 0|2:smem|...]
 
 `matvec` runs the reference matvec demo's loop body (matvecmain.cpp:70-86):

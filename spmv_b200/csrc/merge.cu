@@ -223,7 +223,10 @@ namespace {
 
 // Device address of g_noalloc_carry, looked up once per device (with that
 // device current).  Host code must not use the symbol's name as an address:
-// on the host it names a shadow object, not device memory.
+// on the host it names a shadow object, not device memory.  The cached
+// address belongs to the device's primary context as it was at the first
+// call; a cudaDeviceReset ends that context (and every handle of this
+// library made in it), so the cache is not meant to outlive one.
 void* noalloc_scratch(int device) {
   static std::mutex mu;
   static std::vector<void*> addr;
@@ -256,6 +259,8 @@ extern "C" int spmv_matrix_mult_noalloc(spmv_matrix A, const void* const* x,
     int64_t blocks = 0;
     for (int p = 0; p < a.nparts; ++p) {
       const DevPart& D = C.parts[p];
+      if (D.ncols > 0) require(x[p] != nullptr, "spmv: x vector is NULL");
+      if (D.nrows > 0) require(y[p] != nullptr, "spmv: y vector is NULL");
       const int64_t nb = (int64_t(D.nrows) + D.nnz + TILE - 1) / TILE;
       PartArg& P = a.part[p];
       P.rowptr = C.rowptr.as<int32_t>() + D.rp_off;
