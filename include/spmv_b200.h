@@ -372,28 +372,76 @@ int spmv_cg_block(spmv_matrix A, int nrhs, spmv_memory memory,
 typedef struct spmv_batch_s* spmv_batch;
 
 typedef struct spmv_batch_info {
-  int iterations;   /* inner FP32 CG iterations of this system               */
+  int iterations;   /* inner CG iterations of this right-hand side           */
   int refinements;  /* FP64 true-residual recomputations                     */
   int status;       /* SPMV_SUCCESS or SPMV_ERROR_BREAKDOWN                  */
   int converged;    /* 1 if ||b - A x|| / ||b|| < rtol was confirmed in FP64  */
   double relres;    /* that FP64 relative residual                           */
 } spmv_batch_info;
 
-/* nsys independent SPD systems of sizes n[i] (square CSR blocks, FP64 values;
- * an FP32 copy is made for the inner iterations).  Copies in. */
+/* Inner precision of a batched solve. */
+typedef enum spmv_batch_precision {
+  SPMV_BATCH_MIXED = 0,  /* FP32 inner CG, FP64 refinement (reliable updates)  */
+  SPMV_BATCH_FP64 = 1    /* FP64 CG; the stopping test is confirmed by one
+                            FP64 residual                                       */
+} spmv_batch_precision;
+
+/* Launch shape of the batched kernel (0 in a field of spmv_batch_set_config:
+ * keep the current value). */
+typedef struct spmv_batch_config {
+  int ctas_per_sm;   /* CTAs of 512 threads per SM: 1 or 2                     */
+  int tile_rows;     /* rows a warp takes at a time: 128, 256 or 512           */
+  int rhs_lanes;     /* lanes per block row in the block products: 32 (one
+                        right-hand side per lane) or 16 (two per lane)         */
+  double us;         /* autotune: time of the timed solve, microseconds        */
+  int candidates;    /* autotune: configurations timed (0: from the cache)     */
+} spmv_batch_config;
+
+/* nsys independent SPD systems of sizes n[i] (square CSR blocks with
+ * symmetric patterns, FP64 values) for spmv_batch_solve (no counterpart in
+ * the reference; each solve is spmv::cg's recurrence, cg.cpp:50-80, on
+ * Matrix::operator*, Matrix.cpp:199-204).  Copies in.  At creation each
+ * system is renumbered once (reverse Cuthill-McKee, rows sorted by length in
+ * windows of 1024) and stored as SELL-32 slices with FP32 and FP64 values
+ * and 16-bit column offsets when every offset fits (else 32-bit columns);
+ * the solves map b in and x out.  At most 8191 systems. */
 int spmv_batch_create(spmv_comm comm, int nsys, const int32_t* n,
                       const int32_t* const* rowptr,
                       const int32_t* const* colind,
                       const double* const* values, spmv_batch* batch);
 int spmv_batch_destroy(spmv_batch batch);
-/* CTAs (on different SMs, one thread-block cluster) that share one system:
- * 1, 2, 4 or 8 (default 1). */
-int spmv_batch_set_cluster(spmv_batch batch, int cluster);
+/* System `system` also takes a block of nrhs (1..32) right-hand sides in
+ * spmv_batch_solve_ex, solved in the same launch with one product per
+ * iteration for all its columns (its matrix read once per iteration). */
+int spmv_batch_set_block(spmv_batch batch, int system, int nrhs);
+/* Launch shape; see spmv_batch_config.  spmv_batch_autotune times the
+ * candidates (ctas_per_sm x tile_rows x rhs_lanes) on short solves of this
+ * batch and keeps the fastest; with SPMV_B200_TUNE_CACHE naming a file the
+ * choice is cached by batch statistics. */
+int spmv_batch_set_config(spmv_batch batch, const spmv_batch_config* config);
+int spmv_batch_get_config(spmv_batch batch, spmv_batch_config* config);
+int spmv_batch_autotune(spmv_batch batch, spmv_batch_config* best);
+/* Storage statistics: rows, nonzeros and stored SELL entries (padding
+ * included) over all systems, and the bits per stored column index. */
+int spmv_batch_stats(spmv_batch batch, int64_t* rows, int64_t* nnz,
+                     int64_t* stored, int* index_bits);
 /* Solves every system A_i x_i = b_i to ||b_i - A_i x_i|| / ||b_i|| < rtol
- * (checked in FP64) in one persistent launch: FP32 inner CG iterations with
- * FP64 refinement, as spmv_cg_mixed, one system per thread-block cluster from
- * a work queue ordered largest first.  b[nsys], x[nsys]; info[nsys] may be
- * NULL.  max_its bounds each system's inner iterations. */
+ * (confirmed in FP64) and, when the batch has a block and bblock/xblock are
+ * not NULL, A_s X = B for the block's system s (bblock and xblock n_s x nrhs,
+ * row-major), all in one cooperative launch: every CG iteration of every
+ * system and block column runs in lockstep, each recurrence with its own
+ * alpha, beta and stopping test; a system stops iterating when it has
+ * converged.  precision: SPMV_BATCH_MIXED (FP32 inner iterations, FP64
+ * refinement, as spmv_cg_mixed) or SPMV_BATCH_FP64.  b[nsys], x[nsys];
+ * info[nsys] and block_info[nrhs] may be NULL.  max_its bounds each
+ * recurrence's inner iterations. */
+int spmv_batch_solve_ex(spmv_batch batch, spmv_memory memory,
+                        spmv_batch_precision precision,
+                        const double* const* b, double* const* x,
+                        const double* bblock, double* xblock, int max_its,
+                        double rtol, spmv_batch_info* info,
+                        spmv_batch_info* block_info);
+/* spmv_batch_solve_ex with SPMV_BATCH_MIXED and no block. */
 int spmv_batch_solve(spmv_batch batch, spmv_memory memory,
                      const double* const* b, double* const* x, int max_its,
                      double rtol, spmv_batch_info* info);

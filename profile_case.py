@@ -2,6 +2,7 @@
 
     python profile_case.py --case c2 --reps 3 [--what matvec|cg|mixed]
         [--kernel staged --width 7] [--cg-form 0|2:smem|...]
+    python profile_case.py --what batch --count 24 [--precision mixed|fp64]
 
 `matvec` runs the reference matvec demo's loop body (matvecmain.cpp:70-86):
 L2GMap::update then Matrix::mult over all ranks, `reps` times, as plain
@@ -9,7 +10,9 @@ kernel launches.  `cg` runs one spmv::cg solve: a CUDA graph, or one
 cooperative launch of the fused kernel (`--cg-form` forces the form through
 SPMV_B200_CG_FUSED, so no timing launches precede the solve).  `mixed`
 runs one mixed-precision solve to 1e-10 (`--cg-form` then forces its form
-through SPMV_B200_CG_MIXED_FUSED).
+through SPMV_B200_CG_MIXED_FUSED).  `batch` runs one batched solve (one
+cooperative launch) of the first `count` systems of the batched k-NN
+workload with system 0's 32-column block, to 1e-10.
 """
 from __future__ import annotations
 
@@ -23,7 +26,9 @@ def main():
     ap.add_argument("--case", default="c2")
     ap.add_argument("--scale", type=int, default=0)
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--what", default="matvec", choices=["matvec", "cg", "mixed"])
+    ap.add_argument("--what", default="matvec", choices=["matvec", "cg", "mixed", "batch"])
+    ap.add_argument("--count", type=int, default=24)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--kernel", default="auto", choices=["auto", "vector", "merge", "sell", "staged"])
     ap.add_argument("--width", type=int, default=0)
@@ -37,6 +42,19 @@ def main():
     import torch
     import spmv_b200 as S
     from spmv_b200 import gen
+
+    if args.what == "batch":
+        from spmv_b200.core import Batch
+        systems = gen.c4_systems(count=args.count)
+        comm = S.Comm(size=1, device=0)
+        B = Batch(comm, [(A.rowptr, A.cols, A.vals) for A, _ in systems], block=(0, 32))
+        bs = [torch.from_numpy(b).cuda() for _, b in systems]
+        Bb = torch.from_numpy(gen.c4_block_rhs(systems[0][0].nrows)).cuda()
+        x, info, X, binfo = B.solve(bs, 20000, 1e-10, block_b=Bb, precision=args.precision)
+        print("batch", args.count, "systems", B.stats(), "config", B.config(),
+              "converged", sum(i.converged for i in info) + sum(i.converged for i in binfo),
+              "max iterations", max(i.iterations for i in info + binfo))
+        return
 
     W = gen.workload(args.case, args.scale)
     D = gen.distribute(W.A, W.P)

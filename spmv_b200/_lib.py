@@ -53,6 +53,15 @@ class IrInfo(C.Structure):
 BatchInfo = IrInfo  # same layout as spmv_batch_info
 
 
+class BatchConfig(C.Structure):
+    _fields_ = [("ctas_per_sm", C.c_int), ("tile_rows", C.c_int), ("rhs_lanes", C.c_int),
+                ("us", C.c_double), ("candidates", C.c_int)]
+
+
+BATCH_MIXED = 0
+BATCH_FP64 = 1
+
+
 class TuneResult(C.Structure):
     _fields_ = [("kernel", C.c_int), ("width", C.c_int), ("block", C.c_int),
                 ("us", C.c_double), ("candidates", C.c_int)]
@@ -112,7 +121,14 @@ _SIGS = {
     "spmv_matrix_sample_outer": [_p, _int, C.c_double, _pp, _pp, _pp],
     "spmv_batch_create": [_p, _int, C.POINTER(_i32), _pp, _pp, _pp, C.POINTER(_p)],
     "spmv_batch_destroy": [_p],
-    "spmv_batch_set_cluster": [_p, _int],
+    "spmv_batch_set_block": [_p, _int, _int],
+    "spmv_batch_set_config": [_p, C.POINTER(BatchConfig)],
+    "spmv_batch_get_config": [_p, C.POINTER(BatchConfig)],
+    "spmv_batch_autotune": [_p, C.POINTER(BatchConfig)],
+    "spmv_batch_stats": [_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64),
+                         C.POINTER(_int)],
+    "spmv_batch_solve_ex": [_p, _int, _int, _pp, _pp, _p, _p, _int, C.c_double,
+                            C.POINTER(IrInfo), C.POINTER(IrInfo)],
     "spmv_batch_solve": [_p, _int, _pp, _pp, _int, C.c_double, C.POINTER(IrInfo)],
     "spmv_matrix_autotune": [_p, _int, C.POINTER(TuneResult)],
     "spmv_matrix_cg_form": [_p, C.POINTER(_int), C.POINTER(_int), C.POINTER(_int)],

@@ -484,11 +484,14 @@ def cg_block(comm: Comm, A: Matrix, B: Sequence, max_its: int, rtol: float,
 
 
 class Batch:
-    """Many independent SPD systems (one CSR each) solved together by
-    spmv_batch_solve: one persistent launch, FP32 inner CG with FP64
-    refinement, largest systems first."""
+    """Many independent SPD systems (one CSR each, symmetric pattern) solved
+    together by spmv_batch_solve_ex: one cooperative launch in which every
+    system's CG iterations run in lockstep, FP32 inner iterations with FP64
+    refinement (or plain FP64).  `block=(system, nrhs)` adds a block of nrhs
+    right-hand sides for one system, solved in the same launch with one
+    product per iteration for all its columns."""
 
-    def __init__(self, comm: Comm, systems, cluster: int = 1):
+    def __init__(self, comm: Comm, systems, block: Optional[tuple] = None):
         self.comm = comm
         self._rp = [np.ascontiguousarray(s[0], np.int32) for s in systems]
         self._ci = [np.ascontiguousarray(s[1], np.int32) for s in systems]
@@ -501,21 +504,75 @@ class Batch:
              ptr_array([a.ctypes.data for a in self._ci]),
              ptr_array([a.ctypes.data for a in self._va]), C.byref(h))
         self._h = h
-        self.set_cluster(cluster)
+        # The library keeps its own (renumbered) copy.
+        del self._rp, self._ci, self._va
+        self.block = None
+        if block is not None:
+            self.set_block(*block)
 
-    def set_cluster(self, cluster: int) -> None:
-        call("spmv_batch_set_cluster", self._h, int(cluster))
+    def set_block(self, system: int, nrhs: int) -> None:
+        call("spmv_batch_set_block", self._h, int(system), int(nrhs))
+        self.block = (int(system), int(nrhs))
 
-    def solve(self, b: Sequence, max_its: int, rtol: float, x: Optional[List] = None):
+    def set_config(self, ctas_per_sm: int = 0, tile_rows: int = 0, rhs_lanes: int = 0) -> None:
+        c = _lib.BatchConfig(int(ctas_per_sm), int(tile_rows), int(rhs_lanes), 0.0, 0)
+        call("spmv_batch_set_config", self._h, C.byref(c))
+
+    @staticmethod
+    def _cfg(c) -> dict:
+        return {"ctas_per_sm": c.ctas_per_sm, "tile_rows": c.tile_rows,
+                "rhs_lanes": c.rhs_lanes, "us": c.us, "candidates": c.candidates}
+
+    def config(self) -> dict:
+        c = _lib.BatchConfig()
+        call("spmv_batch_get_config", self._h, C.byref(c))
+        return self._cfg(c)
+
+    def autotune(self) -> dict:
+        """Times the launch shapes on short solves and keeps the fastest."""
+        c = _lib.BatchConfig()
+        call("spmv_batch_autotune", self._h, C.byref(c))
+        return self._cfg(c)
+
+    def stats(self) -> dict:
+        rows, nnz, stored = C.c_int64(), C.c_int64(), C.c_int64()
+        bits = C.c_int()
+        call("spmv_batch_stats", self._h, C.byref(rows), C.byref(nnz), C.byref(stored),
+             C.byref(bits))
+        return {"rows": rows.value, "nnz": nnz.value, "stored": stored.value,
+                "index_bits": bits.value}
+
+    def solve(self, b: Sequence, max_its: int, rtol: float, x: Optional[List] = None,
+              block_b=None, block_x=None, precision: str = "mixed"):
+        """x[i] = A_i^-1 b[i] for every system (and X = A_s^-1 B for the block
+        when block_b is given: n_s x nrhs, row-major).  Returns (x, info) or,
+        with a block, (x, info, X, block_info)."""
         mem, dt, bptrs = _vec_info(b)
         if x is None:
             x = [np.empty_like(v) if not _is_torch(v) else v.new_empty(v.shape) for v in b]
         _, _, xptrs = _vec_info(x)
         info = (_lib.BatchInfo * max(len(b), 1))()
+        binfo = None
+        bb = bx = None
+        if block_b is not None:
+            if self.block is None:
+                raise SpmvError(_lib.ERROR_INVALID_ARGUMENT, "spmv batch: no block was set")
+            if block_x is None:
+                block_x = (np.empty_like(block_b) if not _is_torch(block_b)
+                           else block_b.new_empty(block_b.shape))
+            bm, _, (bb,) = _vec_info([block_b])
+            xm, _, (bx,) = _vec_info([block_x])
+            if bm != mem or xm != mem:
+                raise SpmvError(_lib.ERROR_INVALID_ARGUMENT,
+                                "spmv: mix of host and device vectors")
+            binfo = (_lib.BatchInfo * self.block[1])()
+        prec = {"mixed": _lib.BATCH_MIXED, "fp64": _lib.BATCH_FP64}[precision]
         with self.comm.fence(b):
-            call("spmv_batch_solve", self._h, mem, ptr_array(bptrs), ptr_array(xptrs),
-                 int(max_its), float(rtol), info)
-        return x, list(info)[:len(b)]
+            call("spmv_batch_solve_ex", self._h, mem, prec, ptr_array(bptrs), ptr_array(xptrs),
+                 bb, bx, int(max_its), float(rtol), info, binfo)
+        if block_b is None:
+            return x, list(info)[:len(b)]
+        return x, list(info)[:len(b)], block_x, list(binfo)
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:

@@ -471,9 +471,7 @@ void launch_spmm(spmv_matrix A, int k, const void* const* x, void* const* y,
 void block_cg(spmv_matrix A, int k, const double* d_b, double* d_x, int max_its,
               double rtol, spmv_cg_info* info);
 
-// Persistent batched solve (batch.cu) over the concatenated b and x.
-void batch_solve(spmv_batch B, const double* d_b, double* d_x, int max_its,
-                 double rtol, spmv_batch_info* info);
+
 
 // out[r][k] = scale * lambda[r][row(k)] * x[r][col(k)] (adjoint.cu).
 void launch_sample_outer(spmv_matrix A, double scale, const void* const* lambda,

@@ -251,3 +251,10 @@ def c4_systems(count: int = 256, lo: int = 4096, hi: int = 131072, seed: int = 3
         A = knn_laplacian(n, k, seed, i, shift)
         out.append((A, normal(seed, 300 + i, n)))
     return out
+
+
+def c4_block_rhs(n: int, nrhs: int = 32, seed: int = 3):
+    """The batched workload's block of right-hand sides for system 0:
+    n x nrhs, row-major, column l ~ N(0,1) from stream 400 + l."""
+    return np.ascontiguousarray(np.stack([normal(seed, 400 + l, n) for l in range(nrhs)],
+                                         axis=1))
