@@ -17,7 +17,7 @@ product, timed live over repeated launches of Matrix::mult.
 
 `--impl reference` times the reference's CPU path instead: the oracle's
 restatement of spmv::cg (Eigen/MKL/MPI are not available to build the real
-reference) on all host threads, one bounded sample of CG iterations per step.
+reference) on all host threads, one complete solve per step.
 
 Multi-GPU (torchrun, N > 1): replicas only.  Each rank solves its own copy of
 the workload on its own GPU (no data-path collective); `value` sums solves over
@@ -155,9 +155,30 @@ def barrier(info):
     ranks.barrier(info)
 
 
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_full_solve(W, D, nthreads: int):
+    """One complete oracle spmv::cg solve (cg.cpp:11-83 restated) on
+    `nthreads` host threads; returns (seconds, iterations)."""
+    import oracle
+    om = oracle.Map(D.local_sizes, D.ghosts)
+    b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(D.P)]
+    t0 = time.perf_counter()
+    _, k, _ = oracle.cg(om, D.blocks, b, 10000, W.rtol, nthreads=nthreads)
+    return time.perf_counter() - t0, k
+
+
 def cpu_sample(W, D, budget_s: float, nthreads: int):
-    """Times the oracle's spmv::cg (all host threads) for a bounded number of
-    iterations; returns (seconds per iteration, iterations run)."""
+    """Times the oracle's spmv::cg for a bounded number of iterations (about
+    budget_s seconds); returns (seconds per iteration, iterations run)."""
     import oracle
     om = oracle.Map(D.local_sizes, D.ghosts)
     b = [W.b[D.ranges[q]:D.ranges[q + 1]].copy() for q in range(D.P)]
@@ -201,153 +222,199 @@ def _timed(stream, fn, reps):
     return e0.elapsed_time(e1) / 1e3 / reps, out
 
 
-def run_extras(device: int, reps: int, c4_count: int):
+def run_extras(device: int, reps: int, c4_count: int, which=("c3", "c2", "c4", "c5", "next")):
     """c3: 27-point lognormal Laplacian 160^3 (4,096,000 rows), FP64 CG vs
-    mixed CG, both to ||b - A x|| / ||b|| < 1e-10; the same on the 7-point
-    128^3 Poisson matrix over 8 ranks (the CG workload).  c4: `c4_count` k-NN
-    systems of 4,096..131,072 rows, one batched persistent launch vs one
-    plain FP64 CG solve per system.  c5: one adjoint (forward solve, adjoint
-    solve, dL/dA sampling) on the 1024^2 grid."""
+    mixed CG, both to ||b - A x|| / ||b|| < 1e-10; c2: the same on the
+    7-point 128^3 Poisson matrix over 8 ranks (the CG workload); c4: the
+    batched workload (run_c4); c5: one adjoint (forward solve, adjoint solve,
+    dL/dA sampling) on the 1024^2 grid; next: the rows beyond the CG path.
+    `which` selects the parts."""
     import torch
     import spmv_b200 as S
     from spmv_b200 import gen
     from spmv_b200.core import Batch
     out = {}
-    # c3 ----------------------------------------------------------------------
+    if "c3" in which:
+        t0 = time.perf_counter()
+        W = gen.workload("c3")
+        comm = S.Comm(size=1, device=device)
+        stream = comm.torch_stream()
+        cm = S.L2GMap(comm, [W.A.nrows], [[]])
+        M = S.Matrix(comm, [(W.A.rowptr, W.A.cols, W.A.vals)], cm, cm)
+        tune = M.autotune(reps=5)
+        b = [torch.from_numpy(W.b).cuda(device)]
+        x64 = [torch.zeros_like(b[0])]
+        xm = [torch.zeros_like(b[0])]
+        _, k64 = S.cg(comm, M, b, 20000, 1e-10, x=x64)
+        _, im = S.cg_mixed(comm, M, b, 20000, 1e-10, x=xm)
+        setup_s = time.perf_counter() - t0
+        t64, (_, k64) = _timed(stream, lambda: S.cg(comm, M, b, 20000, 1e-10, x=x64), reps)
+        tmx, (_, im) = _timed(stream, lambda: S.cg_mixed(comm, M, b, 20000, 1e-10, x=xm), reps)
+        r = M.mult(xm)[0]
+        relres_m = float(torch.linalg.norm(b[0] - r) / torch.linalg.norm(b[0]))
+        r = M.mult(x64)[0]
+        relres_64 = float(torch.linalg.norm(b[0] - r) / torch.linalg.norm(b[0]))
+        err = float(torch.linalg.norm(xm[0] - x64[0]) / torch.linalg.norm(x64[0]))
+        out["c3_mixed_vs_fp64"] = {
+            "fp64_cg_solves_per_s": 1.0 / t64, "fp64_iterations": k64,
+            "mixed_solves_per_s": 1.0 / tmx, "mixed_inner_iterations": im.iterations,
+            "mixed_refinements": im.refinements, "speedup": t64 / tmx,
+            "relres_fp64": relres_64, "relres_mixed": relres_m,
+            "error_mixed_vs_fp64_solution": err, "mult_kernel": tune[:3],
+            "cg_product": M.solver_product("cg"),
+            "mixed_products": [M.solver_product("mixed32"), M.solver_product("mixed64")],
+            "cg_form": M.cg_form(), "mixed_form": M.cg_form("mixed"),
+            "setup_s": setup_s}
+        del M, cm, b, x64, xm
+        torch.cuda.empty_cache()
+    if "c2" in which:
+        W = gen.workload("c2")
+        D = gen.distribute(W.A, W.P)
+        comm2 = S.Comm(size=W.P, device=device)
+        stream2 = comm2.torch_stream()
+        cm = S.L2GMap(comm2, D.local_sizes, D.ghosts)
+        rm = S.L2GMap(comm2, D.local_sizes, [[] for _ in range(W.P)])
+        M = S.Matrix(comm2, D.blocks, cm, rm)
+        b = [torch.from_numpy(W.b[D.ranges[q]:D.ranges[q + 1]].copy()).cuda(device)
+             for q in range(W.P)]
+        x64 = [torch.zeros(cm.vec_len(q), dtype=torch.float64, device=f"cuda:{device}")
+               for q in range(W.P)]
+        xm = [torch.zeros_like(v) for v in x64]
+        S.cg(comm2, M, b, 20000, 1e-10, x=x64)
+        S.cg_mixed(comm2, M, b, 20000, 1e-10, x=xm)
+        t64, (_, k64) = _timed(stream2, lambda: S.cg(comm2, M, b, 20000, 1e-10, x=x64), reps)
+        tmx, (_, im) = _timed(stream2, lambda: S.cg_mixed(comm2, M, b, 20000, 1e-10, x=xm), reps)
+        xa = torch.cat([xm[q][:D.local_sizes[q]] for q in range(W.P)])
+        xb = torch.cat([x64[q][:D.local_sizes[q]] for q in range(W.P)])
+        out["c2_mixed_vs_fp64"] = {
+            "fp64_cg_solves_per_s": 1.0 / t64, "fp64_iterations": k64,
+            "mixed_solves_per_s": 1.0 / tmx, "mixed_inner_iterations": im.iterations,
+            "mixed_refinements": im.refinements, "speedup": t64 / tmx,
+            "relres_mixed": im.relres,
+            "error_mixed_vs_fp64_solution": float(torch.linalg.norm(xa - xb) /
+                                                  torch.linalg.norm(xb)),
+            "cg_form": M.cg_form(), "mixed_form": M.cg_form("mixed"),
+            "mixed_products": [M.solver_product("mixed32"), M.solver_product("mixed64")]}
+        del M, cm, rm, b, x64, xm
+        torch.cuda.empty_cache()
+    if "c4" in which:
+        out["c4_batched"] = run_c4(device, reps)
+        torch.cuda.empty_cache()
+    if "c5" in which:
+        from spmv_b200.autograd import SpdSystem, spd_solve
+        G = gen.grid2d_softplus(1024, 1024, 4, 0.5, 1e-3)
+        sysm = SpdSystem(G.rowptr, G.cols, G.vals, device=device, rtol=1e-12)
+        bt = torch.from_numpy(gen.normal(4, 100, G.nrows)).cuda(device)
+        xs = torch.from_numpy(gen.normal(4, 101, G.nrows)).cuda(device)
+        vals = torch.from_numpy(G.vals).cuda(device).requires_grad_(True)
+
+        def adjoint():
+            vals.grad = None
+            x = spd_solve(vals, bt, sysm)
+            L = 0.5 * ((x - xs) ** 2).sum()
+            L.backward()
+            return L
+
+        adjoint()
+        ta, _ = _timed(torch.cuda.current_stream(device), adjoint, 1)
+        out["c5_adjoint"] = {"forward_plus_adjoint_s": ta,
+                             "cg_iterations": sysm.last_iterations[-2:],
+                             "edges": int(2 * 1024 * 1023)}
+        del sysm, bt, xs, vals
+        torch.cuda.empty_cache()
+    if "next" in which:
+        out.update(run_next_rows(device, reps))
+    return out
+
+
+def batch_bytes(ns, nzs, infos, sv, nb=0, nzb=0, binfos=()):
+    """Algorithmic DRAM bytes of one batched solve (value size sv: 4 for the
+    FP32 inner iterations, 8 for FP64; 16-bit column offsets).
+
+    Per inner iteration of a system (n rows, z entries): the product reads
+    the matrix once, z (sv + 2), and p and y once each, 2 n sv; the alpha
+    update reads d, p, r, y and writes d, r, 6 n sv; the p update reads r, p
+    and writes p, 3 n sv.  Per refinement: the FP64 residual reads the FP64
+    matrix, z (8 + 2), x, d, b, p and writes r, n (8 + 8 + 3 sv); the fold
+    reads and writes x and d and the p update moves 3 n sv (counted with the
+    iteration), n (16 + 2 sv).  The block (n_b rows, z_b entries in CSR, 32
+    columns) moves its matrix once per lockstep iteration while any column
+    iterates, z_b (sv + 4) + 4 n_b, and 32 x the per-row vector terms; its
+    refinement events are counted as the largest column refinement count."""
+    total = 0
+    for n, z, inf in zip(ns, nzs, infos):
+        total += inf.iterations * (z * (sv + 2) + 11 * n * sv)
+        total += inf.refinements * (z * (8 + 2) + n * (16 + 3 * sv) + n * (16 + 2 * sv))
+    if binfos:
+        its = max(i.iterations for i in binfos)
+        refs = max(i.refinements for i in binfos)
+        total += its * (nzb * (sv + 4) + 4 * nb + 32 * 11 * nb * sv)
+        total += refs * (nzb * (8 + 4) + 4 * nb + 32 * nb * (16 + 3 * sv + 16 + 2 * sv))
+    return total
+
+
+def run_c4(device: int, reps: int):
+    """The batched workload: 256 k-NN Laplacians of 4,096..131,072 rows and a
+    32-column block of right-hand sides for system 0, every system and column
+    to ||b - A x|| / ||b|| < 1e-10 in one cooperative launch; FP32 inner
+    iterations with FP64 refinement against the same kernel in FP64.  Each
+    precision runs with the launch shape the library's autotuner picks for
+    it."""
+    import torch
+    import spmv_b200 as S
+    from spmv_b200 import gen
+    from spmv_b200.core import Batch
+    hbm, src = peaks()
     t0 = time.perf_counter()
-    W = gen.workload("c3")
+    systems = gen.c4_systems(count=256)
+    gen_s = time.perf_counter() - t0
+    n0 = systems[0][0].nrows
+    Bh = gen.c4_block_rhs(n0)
     comm = S.Comm(size=1, device=device)
     stream = comm.torch_stream()
-    cm = S.L2GMap(comm, [W.A.nrows], [[]])
-    M = S.Matrix(comm, [(W.A.rowptr, W.A.cols, W.A.vals)], cm, cm)
-    tune = M.autotune(reps=5)
-    b = [torch.from_numpy(W.b).cuda(device)]
-    x64 = [torch.zeros_like(b[0])]
-    xm = [torch.zeros_like(b[0])]
-    _, k64 = S.cg(comm, M, b, 20000, 1e-10, x=x64)
-    _, im = S.cg_mixed(comm, M, b, 20000, 1e-10, x=xm)
-    setup_s = time.perf_counter() - t0
-    t64, (_, k64) = _timed(stream, lambda: S.cg(comm, M, b, 20000, 1e-10, x=x64), reps)
-    tmx, (_, im) = _timed(stream, lambda: S.cg_mixed(comm, M, b, 20000, 1e-10, x=xm), reps)
-    r = M.mult(xm)[0]
-    relres_m = float(torch.linalg.norm(b[0] - r) / torch.linalg.norm(b[0]))
-    r = M.mult(x64)[0]
-    relres_64 = float(torch.linalg.norm(b[0] - r) / torch.linalg.norm(b[0]))
-    err = float(torch.linalg.norm(xm[0] - x64[0]) / torch.linalg.norm(x64[0]))
-    out["c3_mixed_vs_fp64"] = {
-        "fp64_cg_solves_per_s": 1.0 / t64, "fp64_iterations": k64,
-        "mixed_solves_per_s": 1.0 / tmx, "mixed_inner_iterations": im.iterations,
-        "mixed_refinements": im.refinements, "speedup": t64 / tmx,
-        "relres_fp64": relres_64, "relres_mixed": relres_m,
-        "error_mixed_vs_fp64_solution": err, "mult_kernel": tune[:3],
-        "cg_product": M.solver_product("cg"),
-        "mixed_products": [M.solver_product("mixed32"), M.solver_product("mixed64")],
-        "cg_form": M.cg_form(), "mixed_form": M.cg_form("mixed"),
-        "setup_s": setup_s}
-    del M, cm, b, x64, xm
-    torch.cuda.empty_cache()
-    # c2 mixed ----------------------------------------------------------------
-    W = gen.workload("c2")
-    D = gen.distribute(W.A, W.P)
-    comm2 = S.Comm(size=W.P, device=device)
-    stream2 = comm2.torch_stream()
-    cm = S.L2GMap(comm2, D.local_sizes, D.ghosts)
-    rm = S.L2GMap(comm2, D.local_sizes, [[] for _ in range(W.P)])
-    M = S.Matrix(comm2, D.blocks, cm, rm)
-    b = [torch.from_numpy(W.b[D.ranges[q]:D.ranges[q + 1]].copy()).cuda(device)
-         for q in range(W.P)]
-    x64 = [torch.zeros(cm.vec_len(q), dtype=torch.float64, device=f"cuda:{device}")
-           for q in range(W.P)]
-    xm = [torch.zeros_like(v) for v in x64]
-    S.cg(comm2, M, b, 20000, 1e-10, x=x64)
-    S.cg_mixed(comm2, M, b, 20000, 1e-10, x=xm)
-    t64, (_, k64) = _timed(stream2, lambda: S.cg(comm2, M, b, 20000, 1e-10, x=x64), reps)
-    tmx, (_, im) = _timed(stream2, lambda: S.cg_mixed(comm2, M, b, 20000, 1e-10, x=xm), reps)
-    xa = torch.cat([xm[q][:D.local_sizes[q]] for q in range(W.P)])
-    xb = torch.cat([x64[q][:D.local_sizes[q]] for q in range(W.P)])
-    out["c2_mixed_vs_fp64"] = {
-        "fp64_cg_solves_per_s": 1.0 / t64, "fp64_iterations": k64,
-        "mixed_solves_per_s": 1.0 / tmx, "mixed_inner_iterations": im.iterations,
-        "mixed_refinements": im.refinements, "speedup": t64 / tmx,
-        "relres_mixed": im.relres,
-        "error_mixed_vs_fp64_solution": float(torch.linalg.norm(xa - xb) /
-                                              torch.linalg.norm(xb)),
-        "cg_form": M.cg_form(), "mixed_form": M.cg_form("mixed"),
-        "mixed_products": [M.solver_product("mixed32"), M.solver_product("mixed64")]}
-    del M, cm, rm, b, x64, xm
-    torch.cuda.empty_cache()
-    # c4 ----------------------------------------------------------------------
     t0 = time.perf_counter()
-    systems = gen.c4_systems(count=c4_count)
-    gen_s = time.perf_counter() - t0
-    comm4 = S.Comm(size=1, device=device)
-    stream4 = comm4.torch_stream()
-    B = Batch(comm4, [(A.rowptr, A.cols, A.vals) for A, _ in systems])
-    bb = [torch.from_numpy(bv).cuda(device) for _, bv in systems]
-    xb = [torch.zeros_like(v) for v in bb]
-    best = None
-    for cl in (1, 2, 4, 8):      # cluster size, picked by timing
-        B.set_cluster(cl)
-        tb, (_, info) = _timed(stream4, lambda: B.solve(bb, 20000, 1e-10, x=xb), 1)
-        if best is None or tb < best[1]:
-            best = (cl, tb)
-    B.set_cluster(best[0])
-    tb, (_, info) = _timed(stream4, lambda: B.solve(bb, 20000, 1e-10, x=xb), reps)
-    conv = sum(int(i.converged) for i in info)
-    worst = max(i.relres for i in info)
-    mats = []
-    for A, _ in systems:
-        c1 = S.L2GMap(comm4, [A.nrows], [[]])
-        mats.append((c1, S.Matrix(comm4, [(A.rowptr, A.cols, A.vals)], c1, c1)))
-    x1 = [torch.zeros_like(v) for v in bb]
-
-    def plain():
-        its = 0
-        for (c1, Mi), bi, xi in zip(mats, bb, x1):
-            _, k = S.cg(comm4, Mi, [bi], 20000, 1e-10, x=[xi])
-            its += k
-        return its
-
-    plain()  # builds the per-system graphs
-    tp, its64 = _timed(stream4, plain, 1)
-    n_rows = sum(A.nrows for A, _ in systems)
-    n_nnz = sum(A.nnz for A, _ in systems)
-    out["c4_batched_vs_fp64"] = {
-        "systems": len(systems), "rows": n_rows, "nnz": n_nnz,
-        "batched_batches_per_s": 1.0 / tb,
-        "batched_system_solves_per_s": len(systems) / tb,
-        "fp64_per_system_system_solves_per_s": len(systems) / tp,
-        "speedup": tp / tb, "cluster": best[0], "converged": conv,
-        "worst_relres": worst, "inner_iterations_total": sum(i.iterations for i in info),
-        "fp64_iterations_total": its64,
-        "h_mean": float(np.mean([A.scalar for A, _ in systems])),
-        "generation_s": gen_s}
-    del mats, B
-    torch.cuda.empty_cache()
-    # c5 ----------------------------------------------------------------------
-    from spmv_b200.autograd import SpdSystem, spd_solve
-    G = gen.grid2d_softplus(1024, 1024, 4, 0.5, 1e-3)
-    sysm = SpdSystem(G.rowptr, G.cols, G.vals, device=device, rtol=1e-12)
-    bt = torch.from_numpy(gen.normal(4, 100, G.nrows)).cuda(device)
-    xs = torch.from_numpy(gen.normal(4, 101, G.nrows)).cuda(device)
-    vals = torch.from_numpy(G.vals).cuda(device).requires_grad_(True)
-
-    def adjoint():
-        vals.grad = None
-        x = spd_solve(vals, bt, sysm)
-        L = 0.5 * ((x - xs) ** 2).sum()
-        L.backward()
-        return L
-
-    adjoint()
-    ta, _ = _timed(torch.cuda.current_stream(device), adjoint, 1)
-    out["c5_adjoint"] = {"forward_plus_adjoint_s": ta,
-                         "cg_iterations": sysm.last_iterations[-2:],
-                         "edges": int(2 * 1024 * 1023)}
-    del sysm, bt, xs, vals
-    torch.cuda.empty_cache()
-    out.update(run_next_rows(device, reps))
-    return out
+    B = Batch(comm, [(A.rowptr, A.cols, A.vals) for A, _ in systems], block=(0, 32))
+    create_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tune = {p: B.autotune(p) for p in ("mixed", "fp64")}
+    tune_s = time.perf_counter() - t0
+    bb = [torch.from_numpy(b).cuda(device) for _, b in systems]
+    Bd = torch.from_numpy(Bh).cuda(device)
+    ns = [A.nrows for A, _ in systems]
+    nzs = [A.nnz for A, _ in systems]
+    nzb = systems[0][0].nnz
+    st = B.stats()
+    res = {}
+    sols = {}
+    for prec, sv in (("mixed", 4), ("fp64", 8)):
+        t, (x, info, X, binfo) = _timed(
+            stream, lambda: B.solve(bb, 20000, 1e-10, block_b=Bd, precision=prec), max(reps, 2))
+        byts = batch_bytes(ns, nzs, info, sv, n0, nzb, binfo)
+        allinfo = list(info) + list(binfo)
+        res[prec] = {
+            "ms_per_launch": t * 1e3, "launches_per_s": 1.0 / t,
+            "rhs_solves_per_s": len(allinfo) / t,
+            "inner_iterations_total": sum(i.iterations for i in allinfo),
+            "refinements_total": sum(i.refinements for i in allinfo),
+            "max_iterations": max(i.iterations for i in allinfo),
+            "converged": sum(int(i.converged) for i in allinfo),
+            "worst_relres": max(i.relres for i in allinfo),
+            "bytes_per_launch": byts, "gbs": byts / t / 1e9,
+            "frac_of_measured_hbm": byts / t / 1e9 / hbm,
+            "config": tune[prec]}
+        sols[prec] = ([v.clone() for v in x], X.clone())
+    err = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+              for a, b in zip(sols["mixed"][0] + [sols["mixed"][1]],
+                              sols["fp64"][0] + [sols["fp64"][1]]))
+    return {"systems": len(systems), "rows": st["rows"], "nnz": st["nnz"],
+            "stored_entries": st["stored"], "index_bits": st["index_bits"],
+            "block": {"system": 0, "rows": n0, "rhs": 32},
+            "rhs_per_launch": len(systems) + 32,
+            "mixed": res["mixed"], "fp64": res["fp64"],
+            "speedup_mixed_vs_fp64": res["fp64"]["ms_per_launch"] / res["mixed"]["ms_per_launch"],
+            "max_rel_diff_mixed_vs_fp64_solution": err,
+            "peak_source": src, "h_mean": float(np.mean([A.scalar for A, _ in systems])),
+            "generation_s": gen_s, "create_s": create_s, "autotune_s": tune_s}
 
 
 def run_next_rows(device: int, reps: int):
@@ -445,6 +512,10 @@ def run_next_rows(device: int, reps: int):
 # Reference arm
 # ---------------------------------------------------------------------------
 def run_reference(args, world, rank):
+    """The reference's CPU path on this host: each step is one complete FP64
+    CG solve of the workload by the oracle's restatement of spmv::cg
+    (cg.cpp:11-83) on all host threads (MKL, Eigen and MPI are not available
+    to build the reference itself)."""
     if rank != 0:
         return
     from spmv_b200 import gen
@@ -452,17 +523,17 @@ def run_reference(args, world, rank):
     W = gen.workload(WORKLOAD)
     D = gen.distribute(W.A, W.P)
     nthreads = oracle.max_threads()
-    k_full = 441  # iterations of the oracle's FP64 CG on this workload
-    per_step = []
+    per_step, its = [], []
     for i in range(args.warmup + args.steps):
-        spi, its = cpu_sample(W, D, args.ref_budget, nthreads)
+        dt, k = cpu_full_solve(W, D, nthreads)
         if i >= args.warmup:
-            per_step.append(spi * k_full)
+            per_step.append(dt)
+            its.append(k)
     t = float(np.mean(per_step))
     value = 1.0 / t
-    sample = ("oracle spmv::cg restatement, %d threads; each step times a bounded "
-              "run of CG iterations (~%.0f s) and scales to the %d iterations of a "
-              "full solve" % (nthreads, args.ref_budget, k_full))
+    sample = ("oracle spmv::cg restatement (reference-restatement CPU, not MKL), "
+              "%d threads on %s: every step one complete solve (%d iterations)"
+              % (nthreads, cpu_model(), its[0]))
     line = {"impl": "reference", "metric": "CG solves/s", "value": value,
             "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t * 1e3,
@@ -470,7 +541,7 @@ def run_reference(args, world, rank):
             "dtype": "f64", "data": "synthetic",
             "config": config_dict(W, D, W.P),
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads,
-                             "kind": "port", "sample": sample},
+                             "kind": "port", "sample": sample, "cpu_model": cpu_model()},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -592,6 +663,7 @@ def run_ours(args, info):
     # "dram_frac" is the matrix stream's bytes over the same time.
     mult_roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                  "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
+                 "traffic_source": "profiles/traffic.json (committed ncu capture)",
                  "kernel": f"{kernel_fn} width={kwidth} block={kblock} "
                            "(Matrix::mult, 8 ranks, one launch)",
                  "bytes_per_launch": kb, "us_per_launch": t_mult * 1e6}
@@ -607,28 +679,44 @@ def run_ours(args, info):
                 cg_traffic = json.loads(tp.read_text()).get("cg_fused_c2")
             except Exception:
                 cg_traffic = None
-        cg_roof = {"bound": "hbm", "achieved": cg_ach, "peak": hbm, "unit": "GB/s",
-                   "frac": cg_ach / hbm, "peak_source": src, "traffic": cg_traffic,
+        # achieved / frac count the compulsory DRAM bytes: the matrix stream
+        # at its stored index width, once per iteration (the CG vectors, 84 MB,
+        # stay in L2 and r in shared memory); the B_iter figure, which counts
+        # vector traffic that never reaches DRAM, is kept as algorithmic_gbs.
+        mat_ach = matrix_bytes / t_launch / 1e9
+        cg_roof = {"bound": "hbm", "achieved": mat_ach, "peak": hbm, "unit": "GB/s",
+                   "frac": mat_ach / hbm, "peak_source": src, "traffic": cg_traffic,
+                   "traffic_source": "profiles/traffic.json: dram__bytes_read.sum + "
+                                     "dram__bytes_write.sum of one launch, committed ncu "
+                                     "capture (not measured in this run)",
                    "kernel": f"cg_fused ({cg_form[1]} CTAs/SM, r in {cg_form[2]}, "
                              f"staged width {cg_w}, {cg_bits}-bit indices; one launch "
                              "per solve)",
-                   "bytes_per_launch": cg_bytes, "us_per_launch": t_launch * 1e6,
-                   "dram_frac": matrix_bytes / t_launch / 1e9 / hbm}
+                   "bytes_per_launch": matrix_bytes, "us_per_launch": t_launch * 1e6,
+                   "bytes_model": "nnz x (8 + index bytes) x iterations",
+                   "algorithmic_gbs": cg_ach, "algorithmic_bytes_per_launch": cg_bytes}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         import oracle
         nth = oracle.max_threads()
-        spi, kk = cpu_sample(W, D, args.cpu_budget, nth)
-        cpu = {"value": 1.0 / (spi * k_mean), "unit": "solves/s", "cores": nth,
-               "kind": "port",
-               "sample": "oracle spmv::cg restatement on %d host threads: %d CG "
-                         "iterations timed (%.1f s), scaled to the %.0f iterations "
-                         "of a full solve" % (nth, kk, spi * kk, k_mean)}
+        dt, kf = cpu_full_solve(W, D, nth)
+        spi1, k1 = cpu_sample(W, D, args.cpu_budget, 1)
+        cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": nth, "kind": "port",
+               "cpu_model": cpu_model(),
+               "sample": "oracle spmv::cg restatement (reference-restatement CPU, not MKL) "
+                         "on %d host threads: one complete solve (%d iterations, %.1f s)"
+                         % (nth, kf, dt),
+               "single_thread": {"value": 1.0 / (spi1 * kf), "unit": "solves/s", "cores": 1,
+                                 "sample": "%d CG iterations at 1 thread (%.1f s; the "
+                                           "reference CI runs OMP_NUM_THREADS=1), scaled to "
+                                           "the %d iterations of a full solve"
+                                           % (k1, spi1 * k1, kf)}}
 
     extras = None
     if world == 1 and not args.no_extras:
-        extras = run_extras(device, args.extra_reps, args.c4_count)
+        extras = run_extras(device, args.extra_reps, args.c4_count,
+                            tuple(args.extras.split(",")))
 
     if rank == 0:
         line = {
@@ -784,6 +872,8 @@ def main():
                     help="skip the c3/c4/c5 mixed, batched and adjoint measurements")
     ap.add_argument("--extra-reps", type=int, default=2)
     ap.add_argument("--c4-count", type=int, default=256)
+    ap.add_argument("--extras", default="c3,c2,c4,c5,next",
+                    help="comma-separated parts of the extras: c3, c2, c4, c5, next")
     ap.add_argument("--table", action="store_true",
                     help="per-configuration CPU/GPU table (c1, c2, c3, c5) instead of the "
                          "benchmark line")

@@ -393,6 +393,9 @@ typedef struct spmv_batch_config {
   int tile_rows;     /* rows a warp takes at a time: 128, 256 or 512           */
   int rhs_lanes;     /* lanes per block row in the block products: 32 (one
                         right-hand side per lane) or 16 (two per lane)         */
+  int window;        /* 2: the products stage the band of the gathered vector
+                        a CTA reads in shared memory; 1: they gather through
+                        L1 (0 in spmv_batch_set_config: keep)                 */
   double us;         /* autotune: time of the timed solve, microseconds        */
   int candidates;    /* autotune: configurations timed (0: from the cache)     */
 } spmv_batch_config;
@@ -414,13 +417,17 @@ int spmv_batch_destroy(spmv_batch batch);
  * spmv_batch_solve_ex, solved in the same launch with one product per
  * iteration for all its columns (its matrix read once per iteration). */
 int spmv_batch_set_block(spmv_batch batch, int system, int nrhs);
-/* Launch shape; see spmv_batch_config.  spmv_batch_autotune times the
- * candidates (ctas_per_sm x tile_rows x rhs_lanes) on short solves of this
- * batch and keeps the fastest; with SPMV_B200_TUNE_CACHE naming a file the
- * choice is cached by batch statistics. */
-int spmv_batch_set_config(spmv_batch batch, const spmv_batch_config* config);
-int spmv_batch_get_config(spmv_batch batch, spmv_batch_config* config);
-int spmv_batch_autotune(spmv_batch batch, spmv_batch_config* best);
+/* Launch shape of the solves of one precision; see spmv_batch_config.
+ * spmv_batch_autotune times the candidates (ctas_per_sm x tile_rows x
+ * rhs_lanes) on short solves of this batch in that precision and keeps the
+ * fastest; with SPMV_B200_TUNE_CACHE naming a file the choice is cached by
+ * batch statistics and precision. */
+int spmv_batch_set_config(spmv_batch batch, spmv_batch_precision precision,
+                          const spmv_batch_config* config);
+int spmv_batch_get_config(spmv_batch batch, spmv_batch_precision precision,
+                          spmv_batch_config* config);
+int spmv_batch_autotune(spmv_batch batch, spmv_batch_precision precision,
+                        spmv_batch_config* best);
 /* Storage statistics: rows, nonzeros and stored SELL entries (padding
  * included) over all systems, and the bits per stored column index. */
 int spmv_batch_stats(spmv_batch batch, int64_t* rows, int64_t* nnz,

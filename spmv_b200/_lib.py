@@ -55,7 +55,7 @@ BatchInfo = IrInfo  # same layout as spmv_batch_info
 
 class BatchConfig(C.Structure):
     _fields_ = [("ctas_per_sm", C.c_int), ("tile_rows", C.c_int), ("rhs_lanes", C.c_int),
-                ("us", C.c_double), ("candidates", C.c_int)]
+                ("window", C.c_int), ("us", C.c_double), ("candidates", C.c_int)]
 
 
 BATCH_MIXED = 0
@@ -122,9 +122,9 @@ _SIGS = {
     "spmv_batch_create": [_p, _int, C.POINTER(_i32), _pp, _pp, _pp, C.POINTER(_p)],
     "spmv_batch_destroy": [_p],
     "spmv_batch_set_block": [_p, _int, _int],
-    "spmv_batch_set_config": [_p, C.POINTER(BatchConfig)],
-    "spmv_batch_get_config": [_p, C.POINTER(BatchConfig)],
-    "spmv_batch_autotune": [_p, C.POINTER(BatchConfig)],
+    "spmv_batch_set_config": [_p, _int, C.POINTER(BatchConfig)],
+    "spmv_batch_get_config": [_p, _int, C.POINTER(BatchConfig)],
+    "spmv_batch_autotune": [_p, _int, C.POINTER(BatchConfig)],
     "spmv_batch_stats": [_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64),
                          C.POINTER(_int)],
     "spmv_batch_solve_ex": [_p, _int, _int, _pp, _pp, _p, _p, _int, C.c_double,

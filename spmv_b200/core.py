@@ -514,24 +514,30 @@ class Batch:
         call("spmv_batch_set_block", self._h, int(system), int(nrhs))
         self.block = (int(system), int(nrhs))
 
-    def set_config(self, ctas_per_sm: int = 0, tile_rows: int = 0, rhs_lanes: int = 0) -> None:
-        c = _lib.BatchConfig(int(ctas_per_sm), int(tile_rows), int(rhs_lanes), 0.0, 0)
-        call("spmv_batch_set_config", self._h, C.byref(c))
+    _PREC = {"mixed": _lib.BATCH_MIXED, "fp64": _lib.BATCH_FP64}
+
+    def set_config(self, ctas_per_sm: int = 0, tile_rows: int = 0, rhs_lanes: int = 0,
+                   window: Optional[bool] = None, precision: str = "mixed") -> None:
+        w = 0 if window is None else (2 if window else 1)
+        c = _lib.BatchConfig(int(ctas_per_sm), int(tile_rows), int(rhs_lanes), w, 0.0, 0)
+        call("spmv_batch_set_config", self._h, self._PREC[precision], C.byref(c))
 
     @staticmethod
     def _cfg(c) -> dict:
         return {"ctas_per_sm": c.ctas_per_sm, "tile_rows": c.tile_rows,
-                "rhs_lanes": c.rhs_lanes, "us": c.us, "candidates": c.candidates}
+                "rhs_lanes": c.rhs_lanes, "window": c.window == 2, "us": c.us,
+                "candidates": c.candidates}
 
-    def config(self) -> dict:
+    def config(self, precision: str = "mixed") -> dict:
         c = _lib.BatchConfig()
-        call("spmv_batch_get_config", self._h, C.byref(c))
+        call("spmv_batch_get_config", self._h, self._PREC[precision], C.byref(c))
         return self._cfg(c)
 
-    def autotune(self) -> dict:
-        """Times the launch shapes on short solves and keeps the fastest."""
+    def autotune(self, precision: str = "mixed") -> dict:
+        """Times the launch shapes on short solves of this precision and keeps
+        the fastest for it."""
         c = _lib.BatchConfig()
-        call("spmv_batch_autotune", self._h, C.byref(c))
+        call("spmv_batch_autotune", self._h, self._PREC[precision], C.byref(c))
         return self._cfg(c)
 
     def stats(self) -> dict:
@@ -566,7 +572,7 @@ class Batch:
                 raise SpmvError(_lib.ERROR_INVALID_ARGUMENT,
                                 "spmv: mix of host and device vectors")
             binfo = (_lib.BatchInfo * self.block[1])()
-        prec = {"mixed": _lib.BATCH_MIXED, "fp64": _lib.BATCH_FP64}[precision]
+        prec = self._PREC[precision]
         with self.comm.fence(b):
             call("spmv_batch_solve_ex", self._h, mem, prec, ptr_array(bptrs), ptr_array(xptrs),
                  bb, bx, int(max_its), float(rtol), info, binfo)

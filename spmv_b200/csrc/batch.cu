@@ -27,8 +27,7 @@ struct spmv_batch_s {
   int block_sys = -1, block_nrhs = 0;
   int32_t block_n = 0, block_npad = 0;
   int64_t block_nnz = 0;
-  LaunchCfg cfg;
-  bool cfg_tuned = false;
+  LaunchCfg cfg[2] = {LaunchCfg{}, LaunchCfg{2, 8, 1, 0}};  // per precision (mixed, FP64)
   int gmax = 0;                   // CTAs of the largest grid (partials are sized for it)
   spmvb::DevBuf units, soff, sbound, vals32, vals64, idx, perm;
   spmvb::DevBuf v32, v64;         // r, p, y, d in FP32 / FP64 (4 x rows_pad)
@@ -55,6 +54,10 @@ unsigned long long wait_ns() {
 int tile_slices_of(int tile_rows) { return tile_rows / 32; }
 
 constexpr int kProfCap = 1 << 16;
+// Refinement test of the mixed solves: refine when the FP32 residual norm has
+// fallen 100x below its largest value since the last refinement (the
+// reliable-update criterion with delta = 0.01; squared norms compared).
+constexpr double kDelta2 = 1e-4;
 // Rows of p the product phase stages per CTA (64 KB in FP32, 96 KB in FP64:
 // two CTAs per SM still fit).
 constexpr int kWinRows32 = 16384;
@@ -197,7 +200,7 @@ void fill_args(spmv_batch B, Args<T, CI>& a, const SolveIo& io, int kmax, double
   a.nrhs = io.with_block ? B->block_nrhs : 0;
   a.soff = B->soff.as<int64_t>();
   a.sbound = B->sbound.as<int2>();
-  a.win_cap = sizeof(T) == 4 ? kWinRows32 : kWinRows64;
+  a.win_cap = cfg.window ? (sizeof(T) == 4 ? kWinRows32 : kWinRows64) : 0;
   a.vals = sizeof(T) == 4 ? reinterpret_cast<const T*>(B->vals32.ptr)
                           : reinterpret_cast<const T*>(B->vals64.ptr);
   a.vals64 = B->vals64.as<double>();
@@ -253,7 +256,7 @@ bool run(spmv_batch B, spmv_batch_precision prec, const SolveIo& io, int kmax, d
   if (prec == SPMV_BATCH_MIXED) {
     if (d16) {
       Args<float, int16_t> a;
-      fill_args(B, a, io, kmax, rtol, 0.01, cfg, dry);
+      fill_args(B, a, io, kmax, rtol, kDelta2, cfg, dry);
       return launch_f32(&a, true, cfg, comm->num_sms, s, dry);
     }
     Args<float, int32_t> a;
@@ -271,19 +274,17 @@ bool run(spmv_batch B, spmv_batch_precision prec, const SolveIo& io, int kmax, d
 }
 
 // The configured shape, or 1 CTA per SM when 2 do not fit.
-LaunchCfg resident_cfg(spmv_batch B, LaunchCfg c, const SolveIo& io) {
+LaunchCfg resident_cfg(spmv_batch B, spmv_batch_precision prec, LaunchCfg c, const SolveIo& io) {
   for (;;) {
-    if (run(B, SPMV_BATCH_MIXED, io, 0, 1.0, c, true) &&
-        run(B, SPMV_BATCH_FP64, io, 0, 1.0, c, true))
-      return c;
+    if (run(B, prec, io, 0, 1.0, c, true)) return c;
     if (c.cps <= 1) fail(SPMV_ERROR_CUDA, "spmv batch: the kernel cannot be made resident");
     c.cps = 1;
   }
 }
 
-std::string tune_key(spmv_batch B) {
+std::string tune_key(spmv_batch B, int prec) {
   std::ostringstream k;
-  k << "batch:v1:" << B->nsys << ":" << B->plan.rows_pad << ":" << B->plan.nnz_total << ":"
+  k << "batch:v3:" << prec << ":" << B->nsys << ":" << B->plan.rows_pad << ":" << B->plan.nnz_total << ":"
     << B->plan.entries << ":" << (B->plan.fits16 ? 16 : 32) << ":" << B->block_nrhs << ":"
     << B->block_n;
   return k.str();
@@ -299,7 +300,7 @@ bool cache_lookup(const std::string& key, LaunchCfg& c, double& us) {
     std::string k;
     LaunchCfg t;
     double u = 0;
-    if ((is >> k >> t.cps >> t.tile_slices >> t.rhs_rows >> u) && k == key) {
+    if ((is >> k >> t.cps >> t.tile_slices >> t.rhs_rows >> t.window >> u) && k == key) {
       c = t;
       us = u;
       return true;
@@ -312,7 +313,8 @@ void cache_store(const std::string& key, const LaunchCfg& c, double us) {
   const char* path = std::getenv("SPMV_B200_TUNE_CACHE");
   if (!path) return;
   std::ofstream f(path, std::ios::app);
-  f << key << " " << c.cps << " " << c.tile_slices << " " << c.rhs_rows << " " << us << "\n";
+  f << key << " " << c.cps << " " << c.tile_slices << " " << c.rhs_rows << " " << c.window << " "
+    << us << "\n";
 }
 
 void check_err(spmv_batch B) {
@@ -478,35 +480,43 @@ int spmv_batch_set_block(spmv_batch B, int system, int nrhs) {
     B->block_npad = npad;
     B->block_nnz = int64_t(bc.size());
     build_units(B);
-    B->cfg_tuned = false;
   });
 }
 
-int spmv_batch_set_config(spmv_batch B, const spmv_batch_config* c) {
+int spmv_batch_set_config(spmv_batch B, spmv_batch_precision prec, const spmv_batch_config* c) {
   return guard([&] {
     require(B != nullptr && c != nullptr, "spmv: NULL argument");
+    require(prec == SPMV_BATCH_MIXED || prec == SPMV_BATCH_FP64, "spmv batch: unknown precision");
+    LaunchCfg& cfg = B->cfg[prec];
     if (c->ctas_per_sm) {
       require(c->ctas_per_sm == 1 || c->ctas_per_sm == 2, "spmv batch: ctas_per_sm must be 1 or 2");
-      B->cfg.cps = c->ctas_per_sm;
+      cfg.cps = c->ctas_per_sm;
     }
     if (c->tile_rows) {
       require(c->tile_rows == 128 || c->tile_rows == 256 || c->tile_rows == 512,
               "spmv batch: tile_rows must be 128, 256 or 512");
-      B->cfg.tile_slices = tile_slices_of(c->tile_rows);
+      cfg.tile_slices = tile_slices_of(c->tile_rows);
     }
     if (c->rhs_lanes) {
       require(c->rhs_lanes == 32 || c->rhs_lanes == 16, "spmv batch: rhs_lanes must be 32 or 16");
-      B->cfg.rhs_rows = 32 / c->rhs_lanes;
+      cfg.rhs_rows = 32 / c->rhs_lanes;
+    }
+    if (c->window) {
+      require(c->window == 1 || c->window == 2, "spmv batch: window must be 1 (off) or 2 (on)");
+      cfg.window = c->window == 2;
     }
   });
 }
 
-int spmv_batch_get_config(spmv_batch B, spmv_batch_config* c) {
+int spmv_batch_get_config(spmv_batch B, spmv_batch_precision prec, spmv_batch_config* c) {
   return guard([&] {
     require(B != nullptr && c != nullptr, "spmv: NULL argument");
-    c->ctas_per_sm = B->cfg.cps;
-    c->tile_rows = 32 * B->cfg.tile_slices;
-    c->rhs_lanes = 32 / B->cfg.rhs_rows;
+    require(prec == SPMV_BATCH_MIXED || prec == SPMV_BATCH_FP64, "spmv batch: unknown precision");
+    const LaunchCfg& cfg = B->cfg[prec];
+    c->ctas_per_sm = cfg.cps;
+    c->tile_rows = 32 * cfg.tile_slices;
+    c->rhs_lanes = 32 / cfg.rhs_rows;
+    c->window = cfg.window ? 2 : 1;
     c->us = 0.0;
     c->candidates = 0;
   });
@@ -525,14 +535,15 @@ int spmv_batch_stats(spmv_batch B, int64_t* rows, int64_t* nnz, int64_t* stored,
   });
 }
 
-int spmv_batch_autotune(spmv_batch B, spmv_batch_config* best) {
+int spmv_batch_autotune(spmv_batch B, spmv_batch_precision prec, spmv_batch_config* best) {
   return guard([&] {
     require(B != nullptr, "spmv: NULL batch");
+    require(prec == SPMV_BATCH_MIXED || prec == SPMV_BATCH_FP64, "spmv batch: unknown precision");
     spmv_comm comm = B->comm;
     comm->require_device();
     DeviceGuard dg(comm->device);
     cudaStream_t s = comm->stream;
-    const std::string key = tune_key(B);
+    const std::string key = tune_key(B, int(prec));
     LaunchCfg pick;
     double pick_us = 0.0;
     int tried = 0;
@@ -567,21 +578,23 @@ int spmv_batch_autotune(spmv_batch B, spmv_batch_config* best) {
       SPMVB_CUDA(cudaEventCreate(&e0));
       SPMVB_CUDA(cudaEventCreate(&e1));
       double best_us = 1e300;
-      const int kmax = 24;
+      const int kmax = 48;
       for (int cps : {2, 1})
         for (int ts : {4, 8, 16})
-          for (int rr : {1, 2}) {
+          for (int rr : {1, 2})
+            for (int win : {1, 0}) {
             if (rr == 2 && !blk) continue;
             LaunchCfg c;
             c.cps = cps;
             c.tile_slices = ts;
             c.rhs_rows = rr;
-            if (!run(B, SPMV_BATCH_MIXED, io, kmax, 1e-30, c, true)) continue;
-            run(B, SPMV_BATCH_MIXED, io, kmax, 1e-30, c, false);
+            c.window = win;
+            if (!run(B, prec, io, kmax, 1e-30, c, true)) continue;
+            run(B, prec, io, kmax, 1e-30, c, false);
             double us = 1e300;
             for (int rep = 0; rep < 2; ++rep) {
               SPMVB_CUDA(cudaEventRecord(e0, s));
-              run(B, SPMV_BATCH_MIXED, io, kmax, 1e-30, c, false);
+              run(B, prec, io, kmax, 1e-30, c, false);
               SPMVB_CUDA(cudaEventRecord(e1, s));
               SPMVB_CUDA(cudaEventSynchronize(e1));
               float ms = 0.f;
@@ -601,12 +614,12 @@ int spmv_batch_autotune(spmv_batch B, spmv_batch_config* best) {
       pick_us = best_us;
       cache_store(key, pick, pick_us);
     }
-    B->cfg = pick;
-    B->cfg_tuned = true;
+    B->cfg[prec] = pick;
     if (best) {
       best->ctas_per_sm = pick.cps;
       best->tile_rows = 32 * pick.tile_slices;
       best->rhs_lanes = 32 / pick.rhs_rows;
+      best->window = pick.window ? 2 : 1;
       best->us = pick_us;
       best->candidates = tried;
     }
@@ -673,7 +686,7 @@ int spmv_batch_solve_ex(spmv_batch B, spmv_memory memory, spmv_batch_precision p
     io.B_user = blk ? Bd : nullptr;
     io.X_user = blk ? Xd : nullptr;
     io.with_block = blk;
-    const LaunchCfg cfg = resident_cfg(B, B->cfg, io);
+    const LaunchCfg cfg = resident_cfg(B, precision, B->cfg[precision], io);
     require(run(B, precision, io, max_its, rtol, cfg, false),
             "spmv batch: the kernel cannot be made resident");
     const int nslot = ns + (blk ? BW : 0);

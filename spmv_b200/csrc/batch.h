@@ -128,6 +128,7 @@ struct LaunchCfg {
   int cps = 2;           // CTAs per SM
   int tile_slices = 8;   // rows per warp tile: 32 x tile_slices (single units)
   int rhs_rows = 1;      // block rows per warp step (lanes per row 32 / rhs_rows)
+  int window = 1;        // products stage the gathered vector in shared memory
 };
 
 // Launch of the lockstep kernel (cooperative; the grid must be resident):

@@ -281,13 +281,14 @@ __device__ __forceinline__ void prefetch_tile(const V* vals, const CI* idx, int6
 // A, single: y = A p over slices s0, s0 + step, ... < s1 of the unit; p.y.
 // Slices are dealt to a CTA's warps round robin, so every warp gets a mix
 // of the wide and narrow slices of the length-sorted windows.  Up to UA
-// entries per lane are in flight (one round for most k-NN rows).
+// entries per lane are in flight (FP32: 16, one round for most k-NN rows;
+// FP64: 8).
 // WIN: p is read from the CTA's shared-memory window, whose element 0 is
 // p[wbase] (global row index); the window covers every column of the slices.
-constexpr int UA = 16;
 template <typename T, typename CI, bool WIN>
 __device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int s0, int step, int s1,
                                     double* ts, int64_t wbase) {
+  constexpr int UA = sizeof(T) == 4 ? 16 : 8;
   const Args<T, CI>& a = x.a;
   const T* pw = reinterpret_cast<const T*>(bat_dyn + win_offset(a.nunits)) - wbase;
   const int lane = int(threadIdx.x) & 31;
@@ -333,45 +334,50 @@ __device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int s0, 
   ts[0] = warp_total(part);
 }
 
-// C, single, refining: r = fl(b - A64 (x + d)); ||r64||^2, r.r, r.p.
-template <typename T, typename CI>
-__device__ __noinline__ void tileC1(const Ctx<T, CI>& x, const Unit& u, int j, double* ts) {
+// C, single, refining: r = fl(b - A64 (x + d)); ||r64||^2, r.r, r.p, over
+// slices s0, s0 + step, ... < s1 (dealt round robin like the product).
+// WIN: x + d (FP64) is read from the CTA's shared-memory window.
+constexpr int UC1 = 8;
+template <typename T, typename CI, bool WIN>
+__device__ __noinline__ void tileC1(const Ctx<T, CI>& x, const Unit& u, int s0, int step, int s1,
+                                    double* ts, int64_t wbase) {
   const Args<T, CI>& a = x.a;
+  const double* xw = reinterpret_cast<const double*>(bat_dyn + win_offset(a.nunits)) - wbase;
   const int lane = int(threadIdx.x) & 31;
-  const int s0 = j * a.tile_slices, s1 = min(u.nslices, s0 + a.tile_slices);
-  const int ns = s1 - s0;
-  const int64_t so = tile_soff(a.soff, u.slice0 + s0, ns);
   const double* __restrict__ vals = a.vals64;
   const CI* __restrict__ idx = a.idx;
-  prefetch_tile(vals, idx, __shfl_sync(0xffffffffu, so, 0), __shfl_sync(0xffffffffu, so, ns));
+  const int nsl = s1 > s0 ? (s1 - s0 + step - 1) / step : 0;
+  int64_t sa = 0, sb = 0;
+  if (lane < nsl) {
+    const int64_t sg = u.slice0 + s0 + int64_t(lane) * step;
+    sa = a.soff[sg];
+    sb = a.soff[sg + 1];
+  }
   double t0 = 0.0, t1 = 0.0, t2 = 0.0;
-  for (int t = 0; t < ns; ++t) {
-    const int64_t e0 = __shfl_sync(0xffffffffu, so, t);
-    const int w = int((__shfl_sync(0xffffffffu, so, t + 1) - e0) >> 5);
-    const int64_t row = u.row0 + 32 * int64_t(s0 + t) + lane;
+  for (int t = 0; t < nsl; ++t) {
+    const int64_t e0 = __shfl_sync(0xffffffffu, sa, t);
+    const int w = int((__shfl_sync(0xffffffffu, sb, t) - e0) >> 5);
+    const int64_t row = u.row0 + 32 * int64_t(s0 + t * step) + lane;
     const double* vp = vals + e0 + lane;
     const CI* ip = idx + e0 + lane;
     double acc = 0.0;
-    for (int k0 = 0; k0 < w; k0 += U / 2) {
-      double v[U / 2], gx[U / 2];
-      T gd[U / 2];
-      int c[U / 2];
+    for (int k0 = 0; k0 < w; k0 += UC1) {
+      double v[UC1];
+      int c[UC1];
 #pragma unroll
-      for (int q = 0; q < U / 2; ++q)
+      for (int q = 0; q < UC1; ++q)
         if (k0 + q < w) {
           v[q] = __ldcs(vp + 32 * (k0 + q));
           c[q] = ldidx(ip + 32 * (k0 + q));
         }
 #pragma unroll
-      for (int q = 0; q < U / 2; ++q)
+      for (int q = 0; q < UC1; ++q)
         if (k0 + q < w) {
           const int64_t cc = gcol<CI>(c[q], row, u.row0);
-          gx[q] = ld_pol(a.x + cc, x.keep);
-          gd[q] = ld_pol(a.d + cc, x.keep);
+          const double xv =
+              WIN ? xw[cc] : ld_pol(a.x + cc, x.keep) + double(ld_pol(a.d + cc, x.keep));
+          acc += v[q] * xv;
         }
-#pragma unroll
-      for (int q = 0; q < U / 2; ++q)
-        if (k0 + q < w) acc += v[q] * (gx[q] + double(gd[q]));
     }
     const double r64 = ld_pol(a.b + row, x.keep) - acc;
     const T rf = T(r64);
@@ -880,99 +886,127 @@ __device__ __noinline__ void tileC2(const Ctx<T, CI>& x, const Unit& u, int j, d
 // (single units: lane 0 for slot0; block: lane l for column l).
 // ---------------------------------------------------------------------------
 // Slot fields go through L2 (another CTA may have written them since this
-// SM last read them).
+// SM last read them).  All lanes of the warp call it; `own` lanes update
+// their slot (lane 0 for a single unit, every lane for the block's
+// columns).  The block's columns refine together: when one of them is due,
+// every active column takes the FP64 residual in the same iteration, since
+// the block's refinement product serves all its columns at once.
 template <typename T, typename CI>
-__device__ __forceinline__ void update_slot(const Ctx<T, CI>& x, int ph, Slot* gsl,
-                                            const double* tot, bool& act, bool& refine) {
+__device__ __forceinline__ void update_slot(const Ctx<T, CI>& x, int ph, Slot* gsl, bool own,
+                                            bool blk, const double* tot, bool& act,
+                                            bool& refine) {
   const Args<T, CI>& a = x.a;
-  Slot local;
-  {
+  Slot L;
+  act = false;
+  refine = false;
+  if (own) {
     const double* src = reinterpret_cast<const double*>(gsl);
-    double* dst = reinterpret_cast<double*>(&local);
+    double* dst = reinterpret_cast<double*>(&L);
 #pragma unroll
     for (int i = 0; i < int(sizeof(Slot) / sizeof(double)); ++i) dst[i] = __ldcg(src + i);
   }
-  Slot* sl = &local;
-  struct Store {
-    Slot* g;
-    const Slot* l;
-    __device__ ~Store() {
-      const double* src = reinterpret_cast<const double*>(l);
-      double* dst = reinterpret_cast<double*>(g);
-#pragma unroll
-      for (int i = 0; i < int(sizeof(Slot) / sizeof(double)); ++i) __stcg(dst + i, src[i]);
-    }
-  } store{gsl, sl};
-  if (ph == PH_INIT) {
+  if (own && ph == PH_INIT) {
     const double rr0 = tot[0];
-    sl->rr0 = rr0;
-    sl->rr = tot[1];
-    sl->rr_max = tot[1];
-    sl->rr_true = rr0;
-    sl->rr_prev = 0.0;
-    sl->alpha = sl->beta = sl->c = 0.0;
-    sl->its = 0;
-    sl->refs = 0;
-    sl->status = SPMV_SUCCESS;
-    sl->converged = rr0 == 0.0;
-    sl->refine_at = -1;
+    L.rr0 = rr0;
+    L.rr = tot[1];
+    L.rr_max = tot[1];
+    L.rr_true = rr0;
+    L.rr_prev = 0.0;
+    L.alpha = L.beta = L.c = 0.0;
+    L.its = 0;
+    L.refs = 0;
+    L.status = SPMV_SUCCESS;
+    L.converged = rr0 == 0.0;
+    L.refine_at = -1;
     act = a.kmax > 0 && rr0 > 0.0 && isfinite(rr0);
-    sl->active = act;
-    refine = false;
-    return;
+    L.active = act;
+  } else if (own && L.active) {
+    act = true;
+    if (ph == PH_A) {
+      const double pap = tot[0];
+      if (pap == 0.0 || !isfinite(pap)) {
+        L.status = SPMV_ERROR_BREAKDOWN;
+        L.active = 0;
+        act = false;
+      } else {
+        L.alpha = L.rr / pap;
+      }
+    } else if (ph == PH_B) {
+      const double rr_new = tot[0];
+      const int its = L.its + 1;
+      L.its = its;
+      const double rr_max = fmax(L.rr_max, rr_new);
+      L.rr_max = rr_max;
+      refine = rr_new < a.delta2 * rr_max || rr_new / L.rr0 < a.rtol2 || its >= a.kmax ||
+               !isfinite(rr_new);
+      L.beta = rr_new / L.rr;
+      L.c = 0.0;
+      L.rr_prev = L.rr;
+      L.rr = rr_new;
+    } else if (ph == PH_C && L.refine_at == x.k) {
+      L.refs += 1;
+      L.rr_true = tot[0];
+      L.rr_max = tot[1];
+      bool stop = false;
+      if (tot[0] / L.rr0 < a.rtol2) {
+        L.converged = 1;
+        stop = true;
+      }
+      if (!isfinite(tot[0])) {
+        L.status = SPMV_ERROR_BREAKDOWN;
+        stop = true;
+      }
+      L.beta = tot[1] / L.rr_prev;
+      L.rr = tot[1];
+      L.c = tot[1] > 0.0 ? tot[2] / tot[1] : 0.0;
+      if (L.its >= a.kmax) stop = true;
+      if (stop) {
+        L.active = 0;
+        act = false;
+      }
+      refine = true;
+    }
   }
-  act = sl->active != 0;
-  refine = false;
-  if (!act) return;
-  if (ph == PH_A) {
-    const double pap = tot[0];
-    if (pap == 0.0 || !isfinite(pap)) {
-      sl->status = SPMV_ERROR_BREAKDOWN;
-      sl->active = 0;
-      act = false;
-    } else {
-      sl->alpha = sl->rr / pap;
-    }
-  } else if (ph == PH_B) {
-    const double rr_new = tot[0];
-    const int its = sl->its + 1;
-    sl->its = its;
-    const double rr_max = fmax(sl->rr_max, rr_new);
-    sl->rr_max = rr_max;
-    refine = rr_new < a.delta2 * rr_max || rr_new / sl->rr0 < a.rtol2 || its >= a.kmax ||
-             !isfinite(rr_new);
-    sl->beta = rr_new / sl->rr;
-    sl->c = 0.0;
-    sl->rr_prev = sl->rr;
-    sl->rr = rr_new;
-    if (refine) sl->refine_at = x.k;
-  } else if (ph == PH_C) {
-    if (sl->refine_at != x.k) return;
-    sl->refs += 1;
-    sl->rr_true = tot[0];
-    sl->rr_max = tot[1];
-    bool stop = false;
-    if (tot[0] / sl->rr0 < a.rtol2) {
-      sl->converged = 1;
-      stop = true;
-    }
-    if (!isfinite(tot[0])) {
-      sl->status = SPMV_ERROR_BREAKDOWN;
-      stop = true;
-    }
-    sl->beta = tot[1] / sl->rr_prev;
-    sl->rr = tot[1];
-    sl->c = tot[1] > 0.0 ? tot[2] / tot[1] : 0.0;
-    if (sl->its >= a.kmax) stop = true;
-    if (stop) {
-      sl->active = 0;
-      act = false;
-    }
-    refine = true;
+  if (ph == PH_B) {
+    if (blk && __ballot_sync(0xffffffffu, refine) != 0u && act) refine = true;
+    if (own && refine) L.refine_at = x.k;
+  }
+  if (own) {
+    const double* src = reinterpret_cast<const double*>(&L);
+    double* dst = reinterpret_cast<double*>(gsl);
+#pragma unroll
+    for (int i = 0; i < int(sizeof(Slot) / sizeof(double)); ++i) __stcg(dst + i, src[i]);
   }
 }
 
 // ---------------------------------------------------------------------------
+// Copies fl64(x + d)[row0 + wlo, row0 + wlo + wsize) into the window (the
+// refinement product's operand).
+template <typename T, typename CI>
+__device__ __forceinline__ void load_window_xd(const Args<T, CI>& a, const Unit& un, int wlo,
+                                               int wsize) {
+  double* win = reinterpret_cast<double*>(bat_dyn + win_offset(a.nunits));
+  const double* xs = a.x + un.row0 + wlo;
+  const T* ds = a.d + un.row0 + wlo;
+  for (int i0 = 4 * int(threadIdx.x); i0 < wsize; i0 += 4 * 2 * NT) {
+    Four<double> xv[2];
+    Four<T> dv[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+      if (i0 + u * 4 * NT < wsize) {
+        xv[u] = ld4(xs + i0 + u * 4 * NT);
+        dv[u] = ld4(ds + i0 + u * 4 * NT);
+      }
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+      if (i0 + u * 4 * NT < wsize) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) xv[u].v[e] = xv[u].v[e] + double(dv[u].v[e]);
+        st4(win + i0 + u * 4 * NT, xv[u]);
+      }
+  }
+}
+
 // One phase over a unit list.
 // ---------------------------------------------------------------------------
 template <int PH, typename T, typename CI, int R>
@@ -996,7 +1030,7 @@ struct NSumOf {
 // result is valid in all.
 template <typename T, typename CI>
 __device__ __forceinline__ bool chunk_window(const Args<T, CI>& a, const Unit& un, int s_lo,
-                                             int s_hi, Smem& sm, int& wlo, int& wsize) {
+                                             int s_hi, Smem& sm, int& wlo, int& wsize, int cap) {
   const int lane = int(threadIdx.x) & 31, warp = int(threadIdx.x) >> 5;
   int lo = 32 * s_lo, hi = 32 * s_hi - 1;
   for (int t = s_lo + int(threadIdx.x); t < s_hi; t += NT) {
@@ -1023,7 +1057,7 @@ __device__ __forceinline__ bool chunk_window(const Args<T, CI>& a, const Unit& u
   }
   wlo = lo & ~3;
   wsize = ((hi + 1 - wlo) + 3) & ~3;
-  return wsize <= a.win_cap;
+  return wsize <= cap;
 }
 
 // Copies p[row0 + wlo, row0 + wlo + wsize) into the window (16-byte steps:
@@ -1140,7 +1174,7 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
     const int nq = sm.nq;
     if (NS > 0) {
       for (int t = int(threadIdx.x); t < nq * NW * NSUM; t += NT) (&sm.sums[0][0][0])[t] = 0.0;
-      if (PH != PH_A)
+      if (PH != PH_A && PH != PH_C)
         for (int t = int(threadIdx.x); t < NW * NSUM * BW; t += NT)
           (&bsum[0][0][0])[t] = 0.0;
       __syncthreads();
@@ -1172,10 +1206,14 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
         }
         if (PH == PH_B) tileB1(x, un, j, ts);
         if (PH == PH_C) {
-          if (sm.q_wt[qq] > 1)
-            tileC1(x, un, j, ts);
-          else
+          if (sm.q_wt[qq] > 1) {
+            if (win)
+              tileC1<T, CI, true>(x, un, j, NW, a_end, ts, wbase);
+            else
+              tileC1<T, CI, false>(x, un, j, NW, a_end, ts, 0);
+          } else {
             tileP1(x, un, j);
+          }
         }
         if (PH == PH_D) tileD1(x, un, j);
         if (PH == PH_FINAL) tileF1(x, un, j);
@@ -1195,10 +1233,12 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
 #pragma unroll
       for (int s = 0; s < NS1; ++s) run[s] += ts[s];
     };
-    if (PH == PH_A) {
-      // Chunks of NW tiles of one unit, one tile per warp; for a single
-      // unit the chunk's window of p is staged in shared memory first.
-      const bool prof = a.prof != nullptr && threadIdx.x == 0;
+    if (PH == PH_A || PH == PH_C) {
+      // Product units in chunks of NW tiles: the chunk's slices are dealt
+      // round robin to the warps, and (single units) the chunk's window of
+      // the gathered vector is staged in shared memory first.  In phase C
+      // the other units' tiles go one per warp in the same loop.
+      const bool prof = PH == PH_A && a.prof != nullptr && threadIdx.x == 0;
       unsigned long long t_a = prof ? gtimer() : 0, t_w = 0, t_l = 0, t_b = 0;
       for (int qq = 0; qq < nq; ++qq) {
         const Unit un = a.units[lu[sm.q_list[qq]]];
@@ -1214,15 +1254,22 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
           bool win = false;
           int wlo = 0, wsize = 0;
           unsigned long long t0 = prof ? gtimer() : 0, t1 = t0, t2 = t0;
-          if (un.kind == 0) {
+          const bool chunked = un.kind == 0 && (PH == PH_A || sm.q_wt[qq] > 1);
+          if (chunked) {
+            const int cap = PH == PH_A ? a.win_cap : a.win_cap * int(sizeof(T)) / 8;
             win = chunk_window(a, un, c0 * a.tile_slices,
-                               min(un.nslices, c1 * a.tile_slices), sm, wlo, wsize);
+                               min(un.nslices, c1 * a.tile_slices), sm, wlo, wsize, cap);
             if (prof) t1 = gtimer();
-            if (win) load_window(a, un, wlo, wsize);
+            if (win) {
+              if (PH == PH_A)
+                load_window(a, un, wlo, wsize);
+              else
+                load_window_xd(a, un, wlo, wsize);
+            }
             __syncthreads();
             if (prof) t2 = gtimer();
           }
-          if (un.kind == 0) {
+          if (chunked) {
             // The chunk's slices, dealt round robin to the warps.
             const int sl0 = c0 * a.tile_slices + warp;
             a_end = min(un.nslices, c1 * a.tile_slices);
@@ -1326,8 +1373,8 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
           }
         }
         bool act = false, refine = false;
-        if (blk || lane == 0)
-          update_slot(x, PH, a.slots + un.slot0 + (blk ? lane : 0), acc, act, refine);
+        update_slot(x, PH, a.slots + un.slot0 + (blk ? lane : 0), blk || lane == 0, blk, acc, act,
+                    refine);
         const unsigned am = __ballot_sync(0xffffffffu, act);
         const unsigned rm = __ballot_sync(0xffffffffu, refine);
         if (lane == 0) {

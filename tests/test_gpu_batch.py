@@ -113,8 +113,9 @@ def test_batch_launch_shapes_agree_and_repeat_bitwise(cuda_device, systems, bloc
     bs = [torch.from_numpy(b.copy()).cuda() for _, b in sub]
     Bd = torch.from_numpy(block_rhs.copy()).cuda()
     ref = None
-    for cps, rows, lanes in [(2, 256, 32), (1, 128, 16), (2, 512, 16), (1, 256, 32)]:
-        B.set_config(cps, rows, lanes)
+    for cps, rows, lanes, win in [(2, 256, 32, True), (1, 128, 16, False), (2, 512, 16, False),
+                                  (1, 256, 32, True)]:
+        B.set_config(cps, rows, lanes, win)
         x, info, X, binfo = B.solve(bs, 20000, RTOL, block_b=Bd)
         xs = [v.cpu().numpy() for v in x]
         for (A, b), xi, inf in zip(sub, xs, info):
@@ -134,9 +135,10 @@ def test_batch_launch_shapes_agree_and_repeat_bitwise(cuda_device, systems, bloc
 
 def test_batch_autotune_picks_a_resident_shape(cuda_device, systems, block_rhs):
     comm, B = make_batch(systems[:2] + [systems[-1]])
-    cfg = B.autotune()
-    assert cfg["candidates"] >= 6 and cfg["us"] > 0
-    assert cfg == {**B.config(), "us": cfg["us"], "candidates": cfg["candidates"]}
+    for prec in ("mixed", "fp64"):
+        cfg = B.autotune(prec)
+        assert cfg["candidates"] >= 6 and cfg["us"] > 0
+        assert cfg == {**B.config(prec), "us": cfg["us"], "candidates": cfg["candidates"]}
     x, info, X, binfo = B.solve([b.copy() for _, b in systems[:2] + [systems[-1]]], 20000,
                                 RTOL, block_b=block_rhs.copy())
     assert all(i.converged == 1 for i in info) and all(i.converged == 1 for i in binfo)
