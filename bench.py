@@ -456,6 +456,41 @@ def run_next_rows(device: int, reps: int):
                                  "kernel": Mc.get_kernel()}
     del Mc, xs, ys, blocks
     torch.cuda.empty_cache()
+    # Restriction: restrictmain.cpp:56-88's loop body on the c2 operator ---
+    # psp = R.transpmult(q) (Matrix.cpp:168-176), then reverse_update(psp)
+    # (L2GMap.cpp:152-170): the ghost entries of each rank's A^T q are added
+    # into their owners.
+    comm = S.Comm(size=P, device=device)
+    stream = comm.torch_stream()
+    cm = S.L2GMap(comm, D.local_sizes, D.ghosts)
+    rm = S.L2GMap(comm, D.local_sizes, [[] for _ in range(P)])
+    Mr = S.Matrix(comm, D.blocks, cm, rm)
+    dev = f"cuda:{device}"
+    qs = [torch.rand(D.local_sizes[r], dtype=torch.float64, device=dev) for r in range(P)]
+    ps = [torch.empty(cm.vec_len(r), dtype=torch.float64, device=dev) for r in range(P)]
+    for _ in range(3):
+        Mr.transpmult(qs, out=ps)
+        cm.reverse_update(ps)
+    nr = max(reps, 50)
+    t_tm, _ = _timed(stream, lambda: Mr.transpmult(qs, out=ps), nr)
+    t_ru, _ = _timed(stream, lambda: cm.reverse_update(ps), nr)
+    t_both, _ = _timed(stream, lambda: (Mr.transpmult(qs, out=ps), cm.reverse_update(ps)), nr)
+    # Algorithmic bytes: A^T as CSR (values, columns, row pointers), q read
+    # once, A^T q written once (owned + ghost entries); reverse_update reads
+    # each ghost value and its owner's entry and writes the owner's entry,
+    # with one 4-byte index per contribution and per target.
+    tb = nnz * 12 + (n + g + P) * 4 + n * 8 + (n + g) * 8
+    rb = g * (8 + 4) + g * (8 + 8 + 4)
+    out["restrict_c2"] = {
+        "transpmult_us": t_tm * 1e6, "transpmult_bytes": tb,
+        "transpmult_gbs": tb / t_tm / 1e9, "transpmult_frac_of_measured_hbm": tb / t_tm / 1e9 / hbm,
+        "reverse_update_us": t_ru * 1e6, "reverse_update_bytes": rb,
+        "reverse_update_gbs": rb / t_ru / 1e9,
+        "transpmult_plus_reverse_update_us": t_both * 1e6,
+        "transpmult_plus_reverse_update_gbs": (tb + rb) / t_both / 1e9,
+        "frac_of_measured_hbm": (tb + rb) / t_both / 1e9 / hbm}
+    del Mr, qs, ps
+    torch.cuda.empty_cache()
     # PETSc reader ----------------------------------------------------------
     with tempfile.TemporaryDirectory() as d:
         fa = f"{d}/A.dat"

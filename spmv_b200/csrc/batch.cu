@@ -442,7 +442,7 @@ int spmv_batch_set_block(spmv_batch B, int system, int nrhs) {
                               cudaMemcpyDeviceToHost));
       }
     }
-    const int32_t npad = (m + 15) / 16 * 16;
+    const int32_t npad = (m + 63) / 64 * 64;  // whole block tiles at every tile size
     std::vector<int32_t> rp(npad + 1, 0), bc;
     std::vector<double> bv64;
     std::vector<float> bv32;
@@ -578,7 +578,7 @@ int spmv_batch_autotune(spmv_batch B, spmv_batch_precision prec, spmv_batch_conf
       SPMVB_CUDA(cudaEventCreate(&e0));
       SPMVB_CUDA(cudaEventCreate(&e1));
       double best_us = 1e300;
-      const int kmax = 48;
+      const int kmax = 64;
       for (int cps : {2, 1})
         for (int ts : {4, 8, 16})
           for (int rr : {1, 2})

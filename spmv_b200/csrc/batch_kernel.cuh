@@ -50,9 +50,24 @@ constexpr int U = 8;  // gathers in flight per lane in the products
 // vector phase).  The FP64 refinement product reads the FP64 matrix and two
 // gathered vectors per entry; the block's refinement product reads its matrix
 // once for all its columns.
+// A block tile holds BT_MUL x tile_slices block rows (32 x that many
+// elements, as many as a single-unit tile of the vector phases).  The
+// weights were set by timing the batched workload's phases: the refinement
+// product is latency-bound (two gathered vectors per entry), and block tiles
+// four times as long were slower in every phase.
+constexpr int BT_MUL = 1;
 __device__ __forceinline__ int tile_weight(int ph, int kind, bool refine) {
-  if (ph == PH_C && refine) return kind == 0 ? 12 : 4;
-  return 1;
+  if (ph == PH_C && refine) return kind == 0 ? 48 : 16 * BT_MUL;
+  return kind == 0 ? 1 : BT_MUL;
+}
+__device__ __forceinline__ int tile_rows_of(const Unit& un, int tile_slices) {
+  return un.kind == 0 ? tile_slices : BT_MUL * tile_slices;
+}
+// Tiles of a unit: 32 x tile_slices rows (single units, nslices slices) or
+// BT_MUL x tile_slices block rows (the block, nslices rows).
+__device__ __forceinline__ int unit_tiles(const Unit& un, int tile_slices) {
+  const int tr = tile_rows_of(un, tile_slices);
+  return (un.nslices + tr - 1) / tr;
 }
 
 struct Smem {
@@ -537,7 +552,8 @@ __device__ __noinline__ void tileF1(const Ctx<T, CI>& x, const Unit& u, int j) {
 // vector).  Column sums are combined over the step's rows and moved to
 // lane = column at the end.
 #define BAT_BROWS(e)                                                      \
-  const int r0_ = j * a.tile_slices, r1_ = min(u.nslices, r0_ + a.tile_slices); \
+  const int r0_ = j * BT_MUL * a.tile_slices,                                   \
+            r1_ = min(u.nslices, r0_ + BT_MUL * a.tile_slices);                   \
   _Pragma("unroll 2") for (int64_t e = int64_t(r0_ + (int(threadIdx.x) & 31) / 8) * BW + \
                                        4 * ((int(threadIdx.x) & 31) % 8);                  \
                            e < int64_t(r1_) * BW; e += 4 * BW)
@@ -570,11 +586,18 @@ __device__ __noinline__ void tileB2(const Ctx<T, CI>& x, const Unit& u, int j, d
   const int c0 = bcol0();
   T af[4];
   bool act[4];
+  double al[4];
+  int ac[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {  // all the loads first: one round trip
+    const Slot* sl = a.slots + u.slot0 + c0 + r;
+    ac[r] = __ldcg(&sl->active);
+    al[r] = __ldcg(&sl->alpha);
+  }
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
-    const Slot* sl = a.slots + u.slot0 + c0 + r;
-    act[r] = __ldcg(&sl->active) != 0;
-    af[r] = act[r] ? T(__ldcg(&sl->alpha)) : T(0);
+    act[r] = ac[r] != 0;
+    af[r] = act[r] ? T(al[r]) : T(0);
   }
   T* __restrict__ dd = a.dB;
   T* __restrict__ rr = a.rB;
@@ -604,11 +627,18 @@ __device__ __noinline__ void tileP2(const Ctx<T, CI>& x, const Unit& u, int j) {
   const int c0 = bcol0();
   T bf[4];
   bool act[4];
+  double be[4];
+  int ac[4];
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const Slot* sl = a.slots + u.slot0 + c0 + r;
-    act[r] = __ldcg(&sl->active) != 0;
-    bf[r] = T(__ldcg(&sl->beta));
+    ac[r] = __ldcg(&sl->active);
+    be[r] = __ldcg(&sl->beta);
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    act[r] = ac[r] != 0;
+    bf[r] = T(be[r]);
   }
   T* __restrict__ pp = a.pB;
   const T* __restrict__ rr = a.rB;
@@ -736,7 +766,7 @@ __device__ __noinline__ void tileA2(const Ctx<T, CI>& x, const Unit& u, int j, d
   const Args<T, CI>& a = x.a;
   constexpr int KW = 32 / R;
   const int lane = int(threadIdx.x) & 31, seg = lane / KW, cl = lane % KW, c0 = cl * R;
-  const int r0 = j * a.tile_slices, r1 = min(u.nslices, r0 + a.tile_slices);
+  const int r0 = j * BT_MUL * a.tile_slices, r1 = min(u.nslices, r0 + BT_MUL * a.tile_slices);
   const T* __restrict__ pB = a.pB;
   double py[R];
 #pragma unroll
@@ -793,9 +823,9 @@ template <typename T, typename CI, int R>
 __device__ __noinline__ void tileC2(const Ctx<T, CI>& x, const Unit& u, int j, double* ts) {
   const Args<T, CI>& a = x.a;
   constexpr int KW = 32 / R;
-  constexpr int UC = U / (2 * R);
+  constexpr int UC = 4;  // entries in flight (each R doubles of x and R of d)
   const int lane = int(threadIdx.x) & 31, seg = lane / KW, cl = lane % KW, c0 = cl * R;
-  const int r0 = j * a.tile_slices, r1 = min(u.nslices, r0 + a.tile_slices);
+  const int r0 = j * BT_MUL * a.tile_slices, r1 = min(u.nslices, r0 + BT_MUL * a.tile_slices);
   bool ref[R], act[R];
   T bf[R];
 #pragma unroll
@@ -1014,7 +1044,7 @@ __device__ __forceinline__ void unit_info(const Args<T, CI>& a, int k, int u, in
                                           int& wt, int& kind) {
   const Unit& un = a.units[u];
   kind = un.kind;
-  ntiles = (un.nslices + a.tile_slices - 1) / a.tile_slices;
+  ntiles = unit_tiles(un, a.tile_slices);
   bool refine = false;
   if (PH == PH_C) refine = __ldcg(&a.ust[u].refine_at) == k;
   wt = tile_weight(PH, kind, refine);
@@ -1428,13 +1458,13 @@ __global__ void __launch_bounds__(NT, 2) lockstep_kernel(const __grid_constant__
   auto all_units = [&](int u, int& w) {
     const Unit& un = a.units[u];
     if (un.n <= 0) return false;
-    w = (un.nslices + a.tile_slices - 1) / a.tile_slices;
+    w = unit_tiles(un, a.tile_slices) * tile_weight(PH_A, un.kind, false);
     return true;
   };
   auto active_units = [&](int u, int& w) {
     if (__ldcg(&a.ust[u].active) == 0) return false;
     const Unit& un = a.units[u];
-    w = (un.nslices + a.tile_slices - 1) / a.tile_slices;
+    w = unit_tiles(un, a.tile_slices) * tile_weight(PH_A, un.kind, false);
     return true;
   };
   int cnt = build_list(a.nunits, lu, lw, sm, all_units);
@@ -1455,7 +1485,7 @@ __global__ void __launch_bounds__(NT, 2) lockstep_kernel(const __grid_constant__
       if (__ldcg(&a.ust[u].active) == 0) return false;
       const Unit& un = a.units[u];
       const bool ref = __ldcg(&a.ust[u].refine_at) == k;
-      w = ((un.nslices + a.tile_slices - 1) / a.tile_slices) * tile_weight(PH_C, un.kind, ref);
+      w = unit_tiles(un, a.tile_slices) * tile_weight(PH_C, un.kind, ref);
       return true;
     });
     // Any unit refining at k?  (the C list holds every active unit)
@@ -1472,7 +1502,7 @@ __global__ void __launch_bounds__(NT, 2) lockstep_kernel(const __grid_constant__
       cnt = build_list(a.nunits, lu, lw, sm, [&](int u, int& w) {
         if (__ldcg(&a.ust[u].refine_at) != k) return false;
         const Unit& un = a.units[u];
-        w = (un.nslices + a.tile_slices - 1) / a.tile_slices;
+        w = unit_tiles(un, a.tile_slices) * tile_weight(PH_A, un.kind, false);
         return true;
       });
       run_phase<PH_D, T, CI, R>(x, cnt, sm.tot >> 20, lu, lw, sm);
