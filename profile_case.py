@@ -3,6 +3,7 @@
     python profile_case.py --case c2 --reps 3 [--what matvec|cg|mixed]
         [--kernel staged --width 7] [--cg-form 0|2:smem|...]
     python profile_case.py --what batch --count 24 [--precision mixed|fp64]
+    python profile_case.py --case c2 --what spmm|bcg|sample|restrict [--nrhs 8]
 
 `matvec` runs the reference matvec demo's loop body (matvecmain.cpp:70-86):
 L2GMap::update then Matrix::mult over all ranks, `reps` times, as plain
@@ -12,7 +13,12 @@ SPMV_B200_CG_FUSED, so no timing launches precede the solve).  `mixed`
 runs one mixed-precision solve to 1e-10 (`--cg-form` then forces its form
 through SPMV_B200_CG_MIXED_FUSED).  `batch` runs one batched solve (one
 cooperative launch) of the first `count` systems of the batched k-NN
-workload with system 0's 32-column block, to 1e-10.
+workload with system 0's 32-column block, to 1e-10.  `spmm` runs
+`reps` block products of `nrhs` right-hand sides (Matrix::operator* on a
+block), `bcg` one block CG solve of `nrhs` columns to the workload's
+tolerance, `sample` `reps` dL/dA samplings (-lambda_i x_j on the pattern),
+`restrict` `reps` passes of transpmult + reverse_update (restrictmain.cpp's
+loop body).
 """
 from __future__ import annotations
 
@@ -26,7 +32,10 @@ def main():
     ap.add_argument("--case", default="c2")
     ap.add_argument("--scale", type=int, default=0)
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--what", default="matvec", choices=["matvec", "cg", "mixed", "batch"])
+    ap.add_argument("--what", default="matvec",
+                    choices=["matvec", "cg", "mixed", "batch", "spmm", "bcg", "sample",
+                             "restrict"])
+    ap.add_argument("--nrhs", type=int, default=8)
     ap.add_argument("--count", type=int, default=24)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
@@ -51,7 +60,7 @@ def main():
         bs = [torch.from_numpy(b).cuda() for _, b in systems]
         Bb = torch.from_numpy(gen.c4_block_rhs(systems[0][0].nrows)).cuda()
         x, info, X, binfo = B.solve(bs, 20000, 1e-10, block_b=Bb, precision=args.precision)
-        print("batch", args.count, "systems", B.stats(), "config", B.config(),
+        print("batch", args.count, "systems", B.stats(), "config", B.config(args.precision),
               "converged", sum(i.converged for i in info) + sum(i.converged for i in binfo),
               "max iterations", max(i.iterations for i in info + binfo))
         return
@@ -80,6 +89,36 @@ def main():
         print("mixed", args.case, "inner iterations", info.iterations, "refinements",
               info.refinements, "form", M.cg_form("mixed"), "products",
               M.solver_product("mixed32"), M.solver_product("mixed64"))
+    elif args.what == "spmm":
+        X = [torch.rand((cm.vec_len(q), args.nrhs), dtype=tdt, device="cuda")
+             for q in range(W.P)]
+        for _ in range(args.reps):
+            Y = M.mult_block(X)
+        comm.synchronize()
+        print("spmm", args.case, "nrhs", args.nrhs, "reps", args.reps)
+    elif args.what == "bcg":
+        Bm = [torch.rand((D.local_sizes[q], args.nrhs), dtype=torch.float64, device="cuda")
+              for q in range(W.P)]
+        from spmv_b200.core import cg_block
+        X, infos = cg_block(comm, M, Bm, 10000, W.rtol)
+        print("bcg", args.case, "nrhs", args.nrhs, "iterations", [i.iterations for i in infos])
+    elif args.what == "sample":
+        lam = [torch.rand(D.local_sizes[q], dtype=torch.float64, device="cuda")
+               for q in range(W.P)]
+        xs = [torch.rand(cm.vec_len(q), dtype=torch.float64, device="cuda") for q in range(W.P)]
+        for _ in range(args.reps):
+            out = M.sample_outer(lam, xs)
+        comm.synchronize()
+        print("sample", args.case, "reps", args.reps)
+    elif args.what == "restrict":
+        qs = [torch.rand(D.local_sizes[q], dtype=torch.float64, device="cuda")
+              for q in range(W.P)]
+        ps = [torch.empty(cm.vec_len(q), dtype=torch.float64, device="cuda") for q in range(W.P)]
+        for _ in range(args.reps):
+            M.transpmult(qs, out=ps)
+            cm.reverse_update(ps)
+        comm.synchronize()
+        print("restrict", args.case, "reps", args.reps)
     else:
         b = [torch.from_numpy(W.b[D.ranges[q]:D.ranges[q + 1]].copy()).cuda()
              for q in range(W.P)]
