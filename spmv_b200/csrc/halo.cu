@@ -38,12 +38,18 @@ __global__ void update_kernel(const __grid_constant__ PtrTable v,
                               const int32_t* __restrict__ ranks,
                               const int32_t* __restrict__ dst,
                               const int32_t* __restrict__ src, int64_t n) {
+  // Launched programmatically: wait for the previous kernel's writes (x may
+  // have just been produced).  Once a CTA has issued its part of the gather
+  // the product that usually follows may be scheduled (it waits for this
+  // kernel's completion before reading anything).
+  pdl_wait();
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x) {
     const int rr = ranks[i];
     const T val = static_cast<const T*>(v.p[rr & 0xffff])[src[i]];
     static_cast<T*>(v.p[rr >> 16])[dst[i]] = val;
   }
+  pdl_launch_dependents();
 }
 
 template <typename T>
@@ -89,12 +95,16 @@ void launch_update(spmv_l2gmap map, spmv_dtype dtype, void* const* vecs,
   const int32_t* rk = H.upd_ranks.as<int32_t>();
   const int32_t* d = H.upd_dst.as<int32_t>();
   const int32_t* s = H.upd_src.as<int32_t>();
+  int64_t n = H.n_update;
+  void* args[] = {const_cast<PtrTable*>(&t), &rk, &d, &s, &n};
+  const void* fn = nullptr;
   switch (dtype) {
-    case SPMV_FLOAT64: update_kernel<double><<<grid, threads, 0, stream>>>(t, rk, d, s, H.n_update); break;
-    case SPMV_FLOAT32: update_kernel<float><<<grid, threads, 0, stream>>>(t, rk, d, s, H.n_update); break;
-    case SPMV_COMPLEX64: update_kernel<C64><<<grid, threads, 0, stream>>>(t, rk, d, s, H.n_update); break;
-    case SPMV_COMPLEX128: update_kernel<C128><<<grid, threads, 0, stream>>>(t, rk, d, s, H.n_update); break;
+    case SPMV_FLOAT64: fn = (const void*)update_kernel<double>; break;
+    case SPMV_FLOAT32: fn = (const void*)update_kernel<float>; break;
+    case SPMV_COMPLEX64: fn = (const void*)update_kernel<C64>; break;
+    case SPMV_COMPLEX128: fn = (const void*)update_kernel<C128>; break;
   }
+  launch_pdl(fn, dim3(grid), dim3(threads), 0, stream, args);
   SPMVB_CUDA(cudaGetLastError());
 }
 

@@ -160,6 +160,23 @@ struct spmv_comm_s {
 
 namespace spmvb {
 
+// Launch with programmatic stream serialization (see pdl_wait in
+// kernels.cuh): the kernel must call pdl_wait() before touching global memory.
+inline void launch_pdl(const void* fn, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       void** args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  SPMVB_CUDA(cudaLaunchKernelExC(&cfg, fn, args));
+}
+
 // Communication pattern of one rank, as L2GMap.cpp:15-122 computes it.
 struct RankMap {
   int64_t local_size = 0;

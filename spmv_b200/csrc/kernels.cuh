@@ -200,6 +200,20 @@ __device__ __forceinline__ void st_pol(float* a, float v, uint64_t pol) {
                : "memory");
 }
 
+// Programmatic dependent launch.  A kernel launched with the
+// programmatic-stream-serialization attribute may start before the kernel
+// ahead of it on the stream has finished; pdl_wait() (griddepcontrol.wait)
+// blocks until that kernel has completed and its memory operations are
+// visible, so a kernel that calls it before its first global-memory access
+// behaves exactly as with an ordinary launch and gains only the overlap of
+// its launch with the previous kernel's tail.  pdl_launch_dependents() lets
+// the next such kernel be scheduled early.  Both are no-ops without the
+// attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Rank owning CTA `b` of a launch (ranks' CTA ranges are ascending).
 __device__ __forceinline__ int find_part(const SpmvArgs& a, int b) {
   int lo = 0, hi = a.nparts - 1;

@@ -382,7 +382,7 @@ void launch_staged_t(const SpmvLaunch& L, const SpmvArgs& a, const DevCsr::Stage
   int ntiles = t.ntiles;
   int* err = L.err;
   void* args[] = {const_cast<SpmvArgs*>(&a), &tiles, &ntiles, &err};
-  SPMVB_CUDA(cudaLaunchKernel(fn, dim3(sh.grid), dim3(SolverStaged::BS), args, size_t(sh.smem), s));
+  launch_pdl(fn, dim3(sh.grid), dim3(SolverStaged::BS), size_t(sh.smem), s, args);
 }
 
 }  // namespace

@@ -298,6 +298,9 @@ __device__ __forceinline__ void sell_staged_rows(const SpmvArgs& a,
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  // A programmatic launch may start during the previous kernel (usually the
+  // ghost gather of L2GMap::update): nothing global is read before it ends.
+  pdl_wait();
 
   if (warp == STAGED_CONSUMERS) {
     // Producer.  The next tile's rank, e0 and n are loaded one tile ahead,
