@@ -33,7 +33,7 @@ CXX = "g++"  # the system compiler (has OpenMP)
 LIB = PKG / "libspmv_b200.so"
 GEN = PKG / "libspmv_gen.so"
 
-CUDA_SOURCES = ["api.cpp", "l2gmap.cpp", "spmv.cu", "merge.cu", "halo.cu", "cg.cu", "ir.cu", "adjoint.cu", "sell.cu", "batch.cu", "batch_plan.cpp", "batch_f32.cu", "batch_f64.cu", "tune.cpp", "block.cu", "petsc.cpp", "assemble.cpp"]
+CUDA_SOURCES = ["api.cpp", "l2gmap.cpp", "spmv.cu", "merge.cu", "halo.cu", "cg.cu", "ir.cu", "adjoint.cu", "sell.cu", "batch.cu", "batch_plan.cpp", "batch_f32.cu", "batch_f64.cu", "tune.cpp", "block.cu", "petsc.cpp", "assemble.cpp", "assemble_dev.cu"]
 HEADERS = ["internal.h", "kernels.cuh", "spmv_kernel.cuh", "sell_staged.cuh", "batch.h",
            "batch_kernel.cuh"]
 

@@ -18,8 +18,8 @@
 //    builds it (:369-428): entries with the same (row, column) are summed in
 //    triplet order, and each row ends up in ascending column order.
 //
-// The assembly is host work on host arrays (as in the reference); the result
-// is uploaded once by spmv_matrix_create_csr.  Where the reference asserts
+// On a communicator with a GPU the assembly runs there (assemble_dev.cu);
+// this file holds the host form, used by communicators without a device.  Where the reference asserts
 // (disabled) or reads out of range - a ghost row owned by its own rank or
 // outside the global range, a column outside the block - this fails with an
 // error.
@@ -187,6 +187,14 @@ struct CplxH {
 
 }  // namespace
 
+// assemble_dev.cu: the same assembly on the communicator's GPU.
+void create_assembled_device(spmv_comm comm, spmv_dtype dtype, const int64_t* nrows_local,
+                             const int64_t* ncols_local, const int32_t* const* rowptr,
+                             const int32_t* const* colind, const void* const* values,
+                             const int64_t* const* row_ghosts, const int64_t* n_row_ghosts,
+                             const int64_t* const* col_ghosts, const int64_t* n_col_ghosts,
+                             spmv_l2gmap* cm, spmv_l2gmap* rm, spmv_matrix* m);
+
 }  // namespace spmvb
 
 using namespace spmvb;
@@ -211,6 +219,16 @@ int spmv_matrix_create_assembled(spmv_comm comm, spmv_dtype dtype, const int64_t
                 n_row_ghosts && col_ghosts && n_col_ghosts,
             "spmv::Matrix::create_matrix - Error: NULL argument");
     spmv_matrix m = nullptr;
+    if (comm->device >= 0) {
+      // Routing, triplet sort and duplicate sums on the GPU.
+      create_assembled_device(comm, dtype, nrows_local, ncols_local, rowptr, colind, values,
+                              row_ghosts, n_row_ghosts, col_ghosts, n_col_ghosts, &cm, &rm, &m);
+      *col_map = cm;
+      *row_map = rm;
+      *A = m;
+      return;
+    }
+    // A communicator without a device (device -1) assembles on the host.
     switch (dtype) {
       case SPMV_FLOAT64:
         create_assembled<double>(comm, dtype, nrows_local, ncols_local, rowptr, colind, values,

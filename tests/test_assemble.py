@@ -135,3 +135,48 @@ def test_assembled_product_and_solve(cuda_device):
     assert abs(k - ko) <= 2
     for r in range(P):
         assert np.linalg.norm(x[r][:nrl[r]] - xo[r][:nrl[r]]) <= 1e-8 * np.linalg.norm(xo[r][:nrl[r]])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("P", [1, 2, 3, 5, 8])
+@pytest.mark.parametrize("dtype", [np.float64, np.complex128, np.float32, np.complex64])
+def test_device_assembly_matches_oracle(cuda_device, P, dtype):
+    """The device assembly (routing, triplet sort, duplicate sums as kernels)
+    is bitwise the oracle's restatement for FP64 types and the host assembly
+    for all types."""
+    blocks, nrl, ncl, rg, cg, G, rr = fem_problem(23, 19, P, dtype, seed=10 + P)
+    M = S.create_matrix(S.Comm(size=P, device=0), blocks, nrl, ncl, rg, cg)
+    H = S.create_matrix(S.Comm(size=P, device=-1), blocks, nrl, ncl, rg, cg)
+    ref = (oracle.create_matrix(blocks, nrl, ncl, rg, cg)
+           if dtype in (np.float64, np.complex128) else None)
+    for r in range(P):
+        rp, ci, va = M.mat(r)
+        hp, hc, hv = H.mat(r)
+        assert np.array_equal(rp, hp) and np.array_equal(ci, hc) and np.array_equal(va, hv)
+        assert np.array_equal(M.col_map().ghosts(r), H.col_map().ghosts(r))
+        if ref is not None:
+            assert np.array_equal(rp, ref[r][0])
+            assert np.array_equal(ci, ref[r][1])
+            assert np.array_equal(va, ref[r][2].astype(dtype))
+            assert np.array_equal(M.col_map().ghosts(r), ref[r][3])
+
+
+@pytest.mark.gpu
+def test_device_assembly_errors(cuda_device):
+    blocks, nrl, ncl, rg, cg, G, rr = fem_problem(6, 5, 2, seed=3)
+    comm = S.Comm(size=2, device=0)
+    bad = [g.copy() for g in rg]
+    bad[1] = np.array([rr[1]] + list(bad[1][1:]), np.int64)
+    with pytest.raises(S.SpmvError, match="owned by its own rank"):
+        S.create_matrix(comm, blocks, nrl, ncl, bad, cg)
+    bcols = [(b[0], b[1].copy(), b[2]) for b in blocks]
+    bcols[0][1][0] = 10**6       # a column outside the block
+    with pytest.raises(S.SpmvError, match="column index outside the block"):
+        S.create_matrix(comm, bcols, nrl, ncl, rg, cg)
+    # An empty rank and a rank without ghost rows.
+    P = 3
+    blocks, nrl, ncl, rg, cg, G, rr = fem_problem(3, 2, P, seed=4)
+    M = S.create_matrix(S.Comm(size=P, device=0), blocks, nrl, ncl, rg, cg)
+    ref = oracle.create_matrix(blocks, nrl, ncl, rg, cg)
+    for r in range(P):
+        assert np.array_equal(M.mat(r)[2], ref[r][2])
