@@ -69,7 +69,7 @@ constexpr int kWinRows64 = 12288;
 void write_profile(spmv_batch B, const char* tag) {
   const char* path = std::getenv("SPMV_B200_BATCH_PROFILE");
   if (!path || !B->prof.ptr) return;
-  std::vector<unsigned long long> h(2 * kProfCap + 16);
+  std::vector<unsigned long long> h(2 * kProfCap + 16 + 3 * 1024);
   SPMVB_CUDA(cudaMemcpy(h.data(), B->prof.ptr, sizeof(unsigned long long) * h.size(),
                         cudaMemcpyDeviceToHost));
   double us[6] = {0, 0, 0, 0, 0, 0};
@@ -95,7 +95,17 @@ void write_profile(spmv_batch B, const char* tag) {
   const double n = sub[5] ? double(sub[5]) : 1.0;
   f << ", \"A_cta_mean_us\": {\"bounds\": " << 1e-3 * sub[0] / n << ", \"load\": "
     << 1e-3 * sub[1] / n << ", \"tiles\": " << 1e-3 * sub[2] / n << ", \"total\": "
-    << 1e-3 * sub[3] / n << ", \"max_total\": " << 1e-3 * sub[4] << "}}\n";
+    << 1e-3 * sub[3] / n << ", \"max_total\": " << 1e-3 * sub[4] << "}";
+  // Per-CTA time in phases A, B, C (microseconds, summed over the solve).
+  const unsigned long long* pc = sub + 16;
+  const char* names[3] = {"A", "B", "C"};
+  for (int ph = 0; ph < 3; ++ph) {
+    f << ", \"cta_" << names[ph] << "_us\": [";
+    for (int c = 0; c < 2 * B->comm->num_sms && c < 1024; ++c)
+      f << (c ? ", " : "") << int64_t(1e-3 * pc[ph * 1024 + c]);
+    f << "]";
+  }
+  f << "}\n";
 }
 
 void upload(DevBuf& buf, const void* src, size_t bytes) {
@@ -197,6 +207,10 @@ void fill_args(spmv_batch B, Args<T, CI>& a, const SolveIo& io, int kmax, double
   a.rtol2 = rtol * rtol;
   a.delta2 = delta2;
   a.tile_slices = cfg.tile_slices;
+  // The block's tiles against single-unit tiles (4), per phase, from per-CTA
+  // phase times on the batched k-NN workload: in FP32 a block tile costs
+  // 0.8x in the product, 1.45x in the alpha update, 1.3x in the p update.
+  a.w = sizeof(T) == 4 ? Weights{6, 12, 10, 128} : Weights{8, 8, 10, 128};
   a.nrhs = io.with_block ? B->block_nrhs : 0;
   a.soff = B->soff.as<int64_t>();
   a.sbound = B->sbound.as<int2>();
@@ -233,8 +247,9 @@ void fill_args(spmv_batch B, Args<T, CI>& a, const SolveIo& io, int kmax, double
   a.prof = nullptr;
   a.prof_cap = 0;
   if (!dry && std::getenv("SPMV_B200_BATCH_PROFILE")) {
-    B->prof.reserve(sizeof(unsigned long long) * (2 * kProfCap + 16));
-    SPMVB_CUDA(cudaMemsetAsync(B->prof.ptr, 0, sizeof(unsigned long long) * (2 * kProfCap + 16),
+    B->prof.reserve(sizeof(unsigned long long) * (2 * kProfCap + 16 + 3 * 1024));
+    SPMVB_CUDA(cudaMemsetAsync(B->prof.ptr, 0,
+                               sizeof(unsigned long long) * (2 * kProfCap + 16 + 3 * 1024),
                                B->comm->stream));
     a.prof = B->prof.as<unsigned long long>();
     a.prof_cap = kProfCap;

@@ -47,6 +47,11 @@ struct UnitState {
   int refine_at;  // lockstep iteration of the unit's latest refinement
 };
 
+// Tile weights of the block unit per phase (a single-unit tile weighs 4).
+struct Weights {
+  int blk_a, blk_b, blk_c, blk_c2;
+};
+
 // Kernel arguments (T: inner precision; CI: int16_t row offsets or int32_t
 // unit-local columns).
 template <typename T, typename CI>
@@ -56,6 +61,7 @@ struct Args {
   int kmax;
   double rtol2, delta2;
   int tile_slices;                 // slices per single-unit tile (= block rows per tile)
+  Weights w;                       // the block's tile weights
   int nrhs;                        // block right-hand sides (0: no block in this solve)
   // Single units (SELL-32 slices, rows in the planned order).
   const int64_t* soff;             // entry offset of each slice (+1 at the end)

@@ -56,9 +56,14 @@ constexpr int U = 8;  // gathers in flight per lane in the products
 // product is latency-bound (two gathered vectors per entry), and block tiles
 // four times as long were slower in every phase.
 constexpr int BT_MUL = 1;
-__device__ __forceinline__ int tile_weight(int ph, int kind, bool refine) {
-  if (ph == PH_C && refine) return kind == 0 ? 48 : 16 * BT_MUL;
-  return kind == 0 ? 1 : BT_MUL;
+// Weights in eighths of a single unit's tile in the same phase (a single
+// unit's refinement tile, an FP64 product plus three sums, counts 48 tiles);
+// the block's weights per phase come with the launch (they differ between
+// the precisions), measured per CTA on the batched workload.
+__device__ __forceinline__ int tile_weight(const Weights& w, int ph, int kind, bool refine) {
+  if (ph == PH_C && refine) return kind == 0 ? 8 * 48 : w.blk_c2;
+  if (kind == 0) return 8;
+  return ph == PH_A ? w.blk_a : ph == PH_B ? w.blk_b : ph == PH_C ? w.blk_c : 8;
 }
 __device__ __forceinline__ int tile_rows_of(const Unit& un, int tile_slices) {
   return un.kind == 0 ? tile_slices : BT_MUL * tile_slices;
@@ -72,13 +77,13 @@ __device__ __forceinline__ int unit_tiles(const Unit& un, int tile_slices) {
 
 struct Smem {
   double sums[MAXQ][NW][NSUM];
-  int q_list[MAXQ], q_ja[MAXQ], q_jb[MAXQ], q_t[MAXQ], q_wt[MAXQ], q_kind[MAXQ];
+  int q_list[MAXQ], q_ja[MAXQ], q_jb[MAXQ], q_t[MAXQ], q_ref[MAXQ], q_kind[MAXQ];
   int q_cf[MAXQ], q_ns[MAXQ];
   int q_pos[MAXQ + 1];
   long long scan[NW];
   long long tot;
   int wmin[NW], wmax[NW];
-  int nq, next_i, nref, ok;
+  int nq, next_i, nref, ok, blk_last;
 };
 
 // Dynamic shared memory: the unit list (2 ints per unit), then a region that
@@ -1041,13 +1046,13 @@ __device__ __forceinline__ void load_window_xd(const Args<T, CI>& a, const Unit&
 // ---------------------------------------------------------------------------
 template <int PH, typename T, typename CI, int R>
 __device__ __forceinline__ void unit_info(const Args<T, CI>& a, int k, int u, int& ntiles,
-                                          int& wt, int& kind) {
+                                          int& wt, int& kind, bool& refine) {
   const Unit& un = a.units[u];
   kind = un.kind;
   ntiles = unit_tiles(un, a.tile_slices);
-  bool refine = false;
+  refine = false;
   if (PH == PH_C) refine = __ldcg(&a.ust[u].refine_at) == k;
-  wt = tile_weight(PH, kind, refine);
+  wt = tile_weight(a.w, PH, kind, refine);
 }
 
 template <int PH>
@@ -1108,6 +1113,32 @@ __device__ __forceinline__ void load_window(const Args<T, CI>& a, const Unit& un
   }
 }
 
+// The recurrence update of a unit whose sums are complete (acc: per lane for
+// the block's columns, in every lane for a single unit), by one warp.
+template <int PH, typename T, typename CI>
+__device__ __forceinline__ void finish_unit(const Ctx<T, CI>& x, int u, const Unit& un, bool blk,
+                                            const double* acc) {
+  const Args<T, CI>& a = x.a;
+  const int lane = int(threadIdx.x) & 31;
+  bool act = false, refine = false;
+  update_slot(x, PH, a.slots + un.slot0 + (blk ? lane : 0), blk || lane == 0, blk, acc, act,
+              refine);
+  const unsigned am = __ballot_sync(0xffffffffu, act);
+  const unsigned rm = __ballot_sync(0xffffffffu, refine);
+  if (lane == 0) {
+    if (PH == PH_INIT) {
+      a.ust[u].active = am != 0;
+      a.ust[u].refine_at = -1;
+    } else if (PH == PH_A || PH == PH_C) {
+      a.ust[u].active = am != 0;
+    } else if (PH == PH_B) {
+      if (rm) a.ust[u].refine_at = x.k;
+    }
+    a.tickets[u] = 0u;
+    __threadfence();
+  }
+}
+
 // One phase over a unit list.  CTA c (of the G' = min(G, W) CTAs that take
 // part) covers weight positions [c W / G', (c + 1) W / G'); every CTA whose
 // range overlaps a unit's tile starts -- the CTAs cta_of(first tile) ..
@@ -1122,6 +1153,18 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
   constexpr int NS1 = NS > 0 ? NS : 1;
   const Args<T, CI>& a = x.a;
   if (cnt == 0 || W <= 0) return;
+  // With a.prof, each CTA adds its time in phases A, B and C (per CTA).
+  struct CtaClock {
+    unsigned long long* slot;
+    unsigned long long t0;
+    __device__ ~CtaClock() {
+      if (slot) atomicAdd(slot, gtimer() - t0);
+    }
+  } cta_clock{(a.prof && threadIdx.x == 0 && (PH == PH_A || PH == PH_B || PH == PH_C))
+                  ? a.prof + 2 * a.prof_cap + 16 + (PH == PH_A ? 0 : PH == PH_B ? 1 : 2) * 1024 +
+                        blockIdx.x
+                  : nullptr,
+              gtimer()};
   const int G = int(W < (long long)gridDim.x ? W : (long long)gridDim.x), cta = int(blockIdx.x);
   if (cta >= G) return;
   const long long Lr = (long long)cta * W / G, Rr = (long long)(cta + 1) * W / G;
@@ -1147,10 +1190,11 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
       while (nq < MAXQ && i < cnt && lw[i] < Rr) {
         const int idx = i + lane;
         int ja = 0, jb = 0, T_ = 0, wt = 1, kind = 0;
+        bool ref = false;
         long long cf = 0, cl = -1;
         const bool in = idx < cnt && lw[idx] < Rr;
         if (in) {
-          unit_info<PH, T, CI, R>(a, x.k, lu[idx], T_, wt, kind);
+          unit_info<PH, T, CI, R>(a, x.k, lu[idx], T_, wt, kind, ref);
           ja = tiles_from(Lr - lw[idx], wt, T_);
           jb = tiles_from(Rr - lw[idx], wt, T_);
           cf = cta_of(lw[idx], W, G);
@@ -1175,7 +1219,7 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
           sm.q_ja[slot] = ja;
           sm.q_jb[slot] = jb;
           sm.q_t[slot] = T_;
-          sm.q_wt[slot] = wt;
+          sm.q_ref[slot] = ref;
           sm.q_kind[slot] = kind;
           sm.q_cf[slot] = int(cf);
           sm.q_ns[slot] = int(cl - cf + 1);
@@ -1236,7 +1280,7 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
         }
         if (PH == PH_B) tileB1(x, un, j, ts);
         if (PH == PH_C) {
-          if (sm.q_wt[qq] > 1) {
+          if (sm.q_ref[qq]) {
             if (win)
               tileC1<T, CI, true>(x, un, j, NW, a_end, ts, wbase);
             else
@@ -1252,7 +1296,7 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
         if (PH == PH_A) tileA2<T, CI, R>(x, un, j, ts);
         if (PH == PH_B) tileB2(x, un, j, ts);
         if (PH == PH_C) {
-          if (sm.q_wt[qq] > 1)
+          if (sm.q_ref[qq])
             tileC2<T, CI, R>(x, un, j, ts);
           else
             tileP2(x, un, j);
@@ -1284,7 +1328,7 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
           bool win = false;
           int wlo = 0, wsize = 0;
           unsigned long long t0 = prof ? gtimer() : 0, t1 = t0, t2 = t0;
-          const bool chunked = un.kind == 0 && (PH == PH_A || sm.q_wt[qq] > 1);
+          const bool chunked = un.kind == 0 && (PH == PH_A || sm.q_ref[qq]);
           if (chunked) {
             const int cap = PH == PH_A ? a.win_cap : a.win_cap * int(sizeof(T)) / 8;
             win = chunk_window(a, un, c0 * a.tile_slices,
@@ -1346,6 +1390,7 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
       if (cur >= 0) flush(cur);
     }
     if (NS > 0) {
+      if (threadIdx.x == 0) sm.blk_last = -1;
       __syncthreads();
       for (int qq = warp; qq < nq; qq += NW) {
         const int u = lu[sm.q_list[qq]];
@@ -1376,6 +1421,12 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
         last = __shfl_sync(0xffffffffu, last, 0);
         if (!last) continue;
         __threadfence();
+        if (blk) {
+          // The block's partials (one per contributing CTA, up to the grid)
+          // are added by the whole CTA below.
+          if (lane == 0) sm.blk_last = qq;
+          continue;
+        }
         double acc[NSUM] = {0.0, 0.0, 0.0};
         if (!blk) {
           for (int sidx = lane; sidx < nslot; sidx += 32) {
@@ -1385,39 +1436,33 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
           }
 #pragma unroll
           for (int s = 0; s < NS; ++s) acc[s] = warp_total(acc[s]);
-        } else {
-          // Eight partials per step in flight, added in slot order.
-          for (int s8 = 0; s8 < nslot; s8 += 8) {
-            double v[8][NS1];
-#pragma unroll
-            for (int t = 0; t < 8; ++t) {
-              const double* src = a.parts + un.part_off + (long long)(s8 + t) * NSUM * BW;
-#pragma unroll
-              for (int s = 0; s < NS; ++s)
-                v[t][s] = s8 + t < nslot ? __ldcg(src + s * BW + lane) : 0.0;
-            }
-#pragma unroll
-            for (int t = 0; t < 8; ++t)
-#pragma unroll
-              for (int s = 0; s < NS; ++s) acc[s] += v[t][s];
-          }
         }
-        bool act = false, refine = false;
-        update_slot(x, PH, a.slots + un.slot0 + (blk ? lane : 0), blk || lane == 0, blk, acc, act,
-                    refine);
-        const unsigned am = __ballot_sync(0xffffffffu, act);
-        const unsigned rm = __ballot_sync(0xffffffffu, refine);
-        if (lane == 0) {
-          if (PH == PH_INIT) {
-            a.ust[u].active = am != 0;
-            a.ust[u].refine_at = -1;
-          } else if (PH == PH_A || PH == PH_C) {
-            a.ust[u].active = am != 0;
-          } else if (PH == PH_B) {
-            if (rm) a.ust[u].refine_at = x.k;
-          }
-          a.tickets[u] = 0u;
-          __threadfence();
+        finish_unit<PH>(x, u, un, blk, acc);
+      }
+      __syncthreads();
+      if (sm.blk_last >= 0) {
+        // Block unit completed by this CTA: warp w adds the partials of
+        // slots w, w + NW, ... (lane = column), then warp 0 adds the warps'
+        // sums in warp order.
+        const int qq = sm.blk_last;
+        const int u = lu[sm.q_list[qq]];
+        const Unit& un = a.units[u];
+        const int nslot = sm.q_ns[qq];
+        double acc[NSUM] = {0.0, 0.0, 0.0};
+        for (int sidx = warp; sidx < nslot; sidx += NW) {
+          const double* src = a.parts + un.part_off + (long long)sidx * NSUM * BW;
+#pragma unroll
+          for (int s = 0; s < NS; ++s) acc[s] += __ldcg(src + s * BW + lane);
+        }
+#pragma unroll
+        for (int s = 0; s < NS; ++s) bsum[warp][s][lane] = acc[s];
+        __syncthreads();
+        if (warp == 0) {
+          double tot[NSUM] = {0.0, 0.0, 0.0};
+          for (int w = 0; w < NW; ++w)
+#pragma unroll
+            for (int s = 0; s < NS; ++s) tot[s] += bsum[w][s][lane];
+          finish_unit<PH>(x, u, un, true, tot);
         }
       }
     }
@@ -1458,13 +1503,19 @@ __global__ void __launch_bounds__(NT, 2) lockstep_kernel(const __grid_constant__
   auto all_units = [&](int u, int& w) {
     const Unit& un = a.units[u];
     if (un.n <= 0) return false;
-    w = unit_tiles(un, a.tile_slices) * tile_weight(PH_A, un.kind, false);
+    w = unit_tiles(un, a.tile_slices) * tile_weight(a.w, PH_INIT, un.kind, false);
     return true;
   };
-  auto active_units = [&](int u, int& w) {
+  auto active_units_a = [&](int u, int& w) {
     if (__ldcg(&a.ust[u].active) == 0) return false;
     const Unit& un = a.units[u];
-    w = unit_tiles(un, a.tile_slices) * tile_weight(PH_A, un.kind, false);
+    w = unit_tiles(un, a.tile_slices) * tile_weight(a.w, PH_A, un.kind, false);
+    return true;
+  };
+  auto active_units_b = [&](int u, int& w) {
+    if (__ldcg(&a.ust[u].active) == 0) return false;
+    const Unit& un = a.units[u];
+    w = unit_tiles(un, a.tile_slices) * tile_weight(a.w, PH_B, un.kind, false);
     return true;
   };
   int cnt = build_list(a.nunits, lu, lw, sm, all_units);
@@ -1472,12 +1523,14 @@ __global__ void __launch_bounds__(NT, 2) lockstep_kernel(const __grid_constant__
   if (!gbar(a, epoch, sm, 1)) return;
   for (int k = 0; k <= a.kmax; ++k) {
     x.k = k;
-    cnt = build_list(a.nunits, lu, lw, sm, active_units);
+    cnt = build_list(a.nunits, lu, lw, sm, active_units_a);
     if (cnt == 0) break;
-    const long long W = sm.tot >> 20;
-    run_phase<PH_A, T, CI, R>(x, cnt, W, lu, lw, sm);
+    run_phase<PH_A, T, CI, R>(x, cnt, sm.tot >> 20, lu, lw, sm);
     if (!gbar(a, epoch, sm, 2)) return;
-    run_phase<PH_B, T, CI, R>(x, cnt, W, lu, lw, sm);
+    // The same units (A's decisions only remove broken-down ones, which B
+    // skips anyway) with B's weights.
+    cnt = build_list(a.nunits, lu, lw, sm, active_units_b);
+    run_phase<PH_B, T, CI, R>(x, cnt, sm.tot >> 20, lu, lw, sm);
     if (!gbar(a, epoch, sm, 3)) return;
     if (threadIdx.x == 0) sm.nref = 0;
     __syncthreads();
@@ -1485,7 +1538,7 @@ __global__ void __launch_bounds__(NT, 2) lockstep_kernel(const __grid_constant__
       if (__ldcg(&a.ust[u].active) == 0) return false;
       const Unit& un = a.units[u];
       const bool ref = __ldcg(&a.ust[u].refine_at) == k;
-      w = unit_tiles(un, a.tile_slices) * tile_weight(PH_C, un.kind, ref);
+      w = unit_tiles(un, a.tile_slices) * tile_weight(a.w, PH_C, un.kind, ref);
       return true;
     });
     // Any unit refining at k?  (the C list holds every active unit)
@@ -1502,7 +1555,7 @@ __global__ void __launch_bounds__(NT, 2) lockstep_kernel(const __grid_constant__
       cnt = build_list(a.nunits, lu, lw, sm, [&](int u, int& w) {
         if (__ldcg(&a.ust[u].refine_at) != k) return false;
         const Unit& un = a.units[u];
-        w = unit_tiles(un, a.tile_slices) * tile_weight(PH_A, un.kind, false);
+        w = unit_tiles(un, a.tile_slices) * tile_weight(a.w, PH_D, un.kind, false);
         return true;
       });
       run_phase<PH_D, T, CI, R>(x, cnt, sm.tot >> 20, lu, lw, sm);
