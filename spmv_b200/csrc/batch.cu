@@ -61,7 +61,7 @@ constexpr double kDelta2 = 1e-4;
 // Rows of p the product phase stages per CTA (64 KB in FP32, 96 KB in FP64:
 // two CTAs per SM still fit).
 constexpr int kWinRows32 = 16384;
-constexpr int kWinRows64 = 12288;
+constexpr int kWinRows64 = 11264;
 
 // With SPMV_B200_BATCH_PROFILE naming a file, each solve appends one line:
 // the time between consecutive grid barriers summed per phase (init, A, B,

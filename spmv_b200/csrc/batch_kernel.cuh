@@ -75,6 +75,9 @@ __device__ __forceinline__ int unit_tiles(const Unit& un, int tile_slices) {
   return (un.nslices + tr - 1) / tr;
 }
 
+// Slices in one chunk of a product unit: NW tiles of at most 16 slices.
+constexpr int CH_MAX = 16 * NW;
+
 struct Smem {
   double sums[MAXQ][NW][NSUM];
   int q_list[MAXQ], q_ja[MAXQ], q_jb[MAXQ], q_t[MAXQ], q_ref[MAXQ], q_kind[MAXQ];
@@ -84,6 +87,11 @@ struct Smem {
   long long tot;
   int wmin[NW], wmax[NW];
   int nq, next_i, nref, ok, blk_last;
+  // The current chunk of a product unit: its slices' entry offsets, the
+  // hand-out counter, and each slice's sums.
+  long long ch_off[CH_MAX + 1];
+  double ch_part[NSUM][CH_MAX];
+  int ch_next;
 };
 
 // Dynamic shared memory: the unit list (2 ints per unit), then a region that
@@ -298,48 +306,69 @@ __device__ __forceinline__ void prefetch_tile(const V* vals, const CI* idx, int6
                : "memory");
 }
 
-// A, single: y = A p over slices s0, s0 + step, ... < s1 of the unit; p.y.
-// Slices are dealt to a CTA's warps round robin, so every warp gets a mix
-// of the wide and narrow slices of the length-sorted windows.  Up to UA
+// A, single: y = A p over the chunk's slices [c_lo, c_hi) of the unit
+// (offsets staged in sm.ch_off), p.y of each slice into sm.ch_part.  The
+// CTA's warps take the slices in order from a shared counter (warp w starts
+// with slice w), so the warps in flight work on neighbouring slices, whose
+// gathers share lines, and no warp is left with the wide slices of the
+// length-sorted windows while the others wait at the chunk's end.  Up to UA
 // entries per lane are in flight (FP32: 16, one round for most k-NN rows;
 // FP64: 8).
 // WIN: p is read from the CTA's shared-memory window, whose element 0 is
 // p[wbase] (global row index); the window covers every column of the slices.
 template <typename T, typename CI, bool WIN>
-__device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int s0, int step, int s1,
-                                    double* ts, int64_t wbase) {
+__device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int c_lo, int c_hi,
+                                    int64_t wbase, Smem& sm) {
   constexpr int UA = sizeof(T) == 4 ? 16 : 8;
+  constexpr int UT = sizeof(T) == 4 ? UA / 4 : 0;
   const Args<T, CI>& a = x.a;
   const T* pw = reinterpret_cast<const T*>(bat_dyn + win_offset(a.nunits)) - wbase;
   const int lane = int(threadIdx.x) & 31;
   const T* __restrict__ vals = a.vals;
   const CI* __restrict__ idx = a.idx;
   const T* __restrict__ pv_ = a.p;
-  // Lane l holds the entry range of the warp's slice l.
-  const int nsl = s1 > s0 ? (s1 - s0 + step - 1) / step : 0;
-  int64_t sa = 0, sb = 0;
-  if (lane < nsl) {
-    const int64_t sg = u.slice0 + s0 + int64_t(lane) * step;
-    sa = a.soff[sg];
-    sb = a.soff[sg + 1];
-  }
-  double part = 0.0;
-  for (int t = 0; t < nsl; ++t) {
-    const int64_t e0 = __shfl_sync(0xffffffffu, sa, t);
-    const int w = int((__shfl_sync(0xffffffffu, sb, t) - e0) >> 5);
-    const int64_t row = u.row0 + 32 * int64_t(s0 + t * step) + lane;
+  const int n = c_hi - c_lo;
+  int i = int(threadIdx.x) >> 5;
+  while (i < n) {
+    // The next slice is claimed while this one streams.
+    int nxt = 0;
+    if (lane == 0) nxt = atomicAdd(&sm.ch_next, 1);
+    const int64_t e0 = sm.ch_off[i];
+    const int w = int((sm.ch_off[i + 1] - e0) >> 5);
+    const int64_t row = u.row0 + 32 * int64_t(c_lo + i) + lane;
     const T* vp = vals + e0 + lane;
     const CI* ip = idx + e0 + lane;
     T acc = T(0);
+    // Every lane loads UA entries (past the slice's width it repeats the last
+    // one, so no predicate stays live across the loads and the batch fits the
+    // registers); only the slice's own entries gather p.  FP32: a remainder of
+    // at most UA / 4 entries takes a short batch.
     for (int k0 = 0; k0 < w; k0 += UA) {
+      if (UT > 0 && w - k0 <= UT) {
+        T v[UT > 0 ? UT : 1];
+        int c[UT > 0 ? UT : 1];
+#pragma unroll
+        for (int q = 0; q < UT; ++q) {
+          const int kk = min(k0 + q, w - 1);
+          v[q] = __ldcs(vp + 32 * kk);
+          c[q] = ldidx(ip + 32 * kk);
+        }
+#pragma unroll
+        for (int q = 0; q < UT; ++q)
+          if (k0 + q < w) {
+            const int64_t gc = gcol<CI>(c[q], row, u.row0);
+            acc += v[q] * (WIN ? pw[gc] : ld_pol(pv_ + gc, x.keep));
+          }
+        break;
+      }
       T v[UA];
       int c[UA];
 #pragma unroll
-      for (int q = 0; q < UA; ++q)
-        if (k0 + q < w) {
-          v[q] = __ldcs(vp + 32 * (k0 + q));
-          c[q] = ldidx(ip + 32 * (k0 + q));
-        }
+      for (int q = 0; q < UA; ++q) {
+        const int kk = min(k0 + q, w - 1);
+        v[q] = __ldcs(vp + 32 * kk);
+        c[q] = ldidx(ip + 32 * kk);
+      }
 #pragma unroll
       for (int q = 0; q < UA; ++q)
         if (k0 + q < w) {
@@ -349,35 +378,32 @@ __device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int s0, 
     }
     st_pol(a.y + row, acc, x.keep);
     const T pv = WIN ? pw[row] : ld_pol(pv_ + row, x.keep);
-    part += double(pv) * double(acc);
+    const double part = warp_total(double(pv) * double(acc));
+    if (lane == 0) sm.ch_part[0][i] = part;
+    i = __shfl_sync(0xffffffffu, nxt, 0);
   }
-  ts[0] = warp_total(part);
 }
 
-// C, single, refining: r = fl(b - A64 (x + d)); ||r64||^2, r.r, r.p, over
-// slices s0, s0 + step, ... < s1 (dealt round robin like the product).
+// C, single, refining: r = fl(b - A64 (x + d)); ||r64||^2, r.r, r.p per
+// slice of the chunk [c_lo, c_hi) (handed out like the product's).
 // WIN: x + d (FP64) is read from the CTA's shared-memory window.
 constexpr int UC1 = 8;
 template <typename T, typename CI, bool WIN>
-__device__ __noinline__ void tileC1(const Ctx<T, CI>& x, const Unit& u, int s0, int step, int s1,
-                                    double* ts, int64_t wbase) {
+__device__ __noinline__ void tileC1(const Ctx<T, CI>& x, const Unit& u, int c_lo, int c_hi,
+                                    int64_t wbase, Smem& sm) {
   const Args<T, CI>& a = x.a;
   const double* xw = reinterpret_cast<const double*>(bat_dyn + win_offset(a.nunits)) - wbase;
   const int lane = int(threadIdx.x) & 31;
   const double* __restrict__ vals = a.vals64;
   const CI* __restrict__ idx = a.idx;
-  const int nsl = s1 > s0 ? (s1 - s0 + step - 1) / step : 0;
-  int64_t sa = 0, sb = 0;
-  if (lane < nsl) {
-    const int64_t sg = u.slice0 + s0 + int64_t(lane) * step;
-    sa = a.soff[sg];
-    sb = a.soff[sg + 1];
-  }
-  double t0 = 0.0, t1 = 0.0, t2 = 0.0;
-  for (int t = 0; t < nsl; ++t) {
-    const int64_t e0 = __shfl_sync(0xffffffffu, sa, t);
-    const int w = int((__shfl_sync(0xffffffffu, sb, t) - e0) >> 5);
-    const int64_t row = u.row0 + 32 * int64_t(s0 + t * step) + lane;
+  const int n = c_hi - c_lo;
+  int i = int(threadIdx.x) >> 5;
+  while (i < n) {
+    int nxt = 0;
+    if (lane == 0) nxt = atomicAdd(&sm.ch_next, 1);
+    const int64_t e0 = sm.ch_off[i];
+    const int w = int((sm.ch_off[i + 1] - e0) >> 5);
+    const int64_t row = u.row0 + 32 * int64_t(c_lo + i) + lane;
     const double* vp = vals + e0 + lane;
     const CI* ip = idx + e0 + lane;
     double acc = 0.0;
@@ -385,31 +411,32 @@ __device__ __noinline__ void tileC1(const Ctx<T, CI>& x, const Unit& u, int s0, 
       double v[UC1];
       int c[UC1];
 #pragma unroll
-      for (int q = 0; q < UC1; ++q)
-        if (k0 + q < w) {
-          v[q] = __ldcs(vp + 32 * (k0 + q));
-          c[q] = ldidx(ip + 32 * (k0 + q));
-        }
+      for (int q = 0; q < UC1; ++q) {
+        const int kk = min(k0 + q, w - 1);
+        v[q] = __ldcs(vp + 32 * kk);
+        c[q] = ldidx(ip + 32 * kk);
+      }
 #pragma unroll
       for (int q = 0; q < UC1; ++q)
         if (k0 + q < w) {
           const int64_t cc = gcol<CI>(c[q], row, u.row0);
-          const double xv =
-              WIN ? xw[cc] : ld_pol(a.x + cc, x.keep) + double(ld_pol(a.d + cc, x.keep));
-          acc += v[q] * xv;
+          acc += v[q] * (WIN ? xw[cc] : ld_pol(a.x + cc, x.keep) + double(ld_pol(a.d + cc, x.keep)));
         }
     }
     const double r64 = ld_pol(a.b + row, x.keep) - acc;
     const T rf = T(r64);
     st_pol(a.r + row, rf, x.keep);
     const T pv = ld_pol(a.p + row, x.keep);
-    t0 += r64 * r64;
-    t1 += double(rf) * double(rf);
-    t2 += double(rf) * double(pv);
+    const double t0 = warp_total(r64 * r64);
+    const double t1 = warp_total(double(rf) * double(rf));
+    const double t2 = warp_total(double(rf) * double(pv));
+    if (lane == 0) {
+      sm.ch_part[0][i] = t0;
+      sm.ch_part[1][i] = t1;
+      sm.ch_part[2][i] = t2;
+    }
+    i = __shfl_sync(0xffffffffu, nxt, 0);
   }
-  ts[0] = warp_total(t0);
-  ts[1] = warp_total(t1);
-  ts[2] = warp_total(t2);
 }
 
 // Rows of a single-unit tile for the vector phases: 4 consecutive rows per
@@ -799,9 +826,11 @@ __device__ __noinline__ void tileA2(const Ctx<T, CI>& x, const Unit& u, int j, d
           c[q] = __shfl_sync(0xffffffffu, cj, (t0 + q) % KW, KW);
           v[q] = __shfl_sync(0xffffffffu, vj, (t0 + q) % KW, KW);
         }
+        // Every index is a valid row (0 for a missing entry, another entry's
+        // column past cnt), so the gathers need no predicate; the sum takes
+        // the first cnt.
 #pragma unroll
-        for (int q = 0; q < U; ++q)
-          if (t0 + q < cnt) ldR<T, R>(pB + int64_t(c[q]) * BW + c0, g[q]);
+        for (int q = 0; q < U; ++q) ldR<T, R>(pB + int64_t(c[q]) * BW + c0, g[q]);
 #pragma unroll
         for (int q = 0; q < U; ++q)
           if (t0 + q < cnt)
@@ -867,11 +896,10 @@ __device__ __noinline__ void tileC2(const Ctx<T, CI>& x, const Unit& u, int j, d
           v[q] = __shfl_sync(0xffffffffu, vj, (t0i + q) % KW, KW);
         }
 #pragma unroll
-        for (int q = 0; q < UC; ++q)
-          if (t0i + q < cnt) {
-            ldR<double, R>(a.xB + int64_t(c[q]) * BW + c0, gx[q]);
-            ldR<T, R>(a.dB + int64_t(c[q]) * BW + c0, gd[q]);
-          }
+        for (int q = 0; q < UC; ++q) {
+          ldR<double, R>(a.xB + int64_t(c[q]) * BW + c0, gx[q]);
+          ldR<T, R>(a.dB + int64_t(c[q]) * BW + c0, gd[q]);
+        }
 #pragma unroll
         for (int q = 0; q < UC; ++q)
           if (t0i + q < cnt)
@@ -1068,11 +1096,14 @@ __device__ __forceinline__ bool chunk_window(const Args<T, CI>& a, const Unit& u
                                              int s_hi, Smem& sm, int& wlo, int& wsize, int cap) {
   const int lane = int(threadIdx.x) & 31, warp = int(threadIdx.x) >> 5;
   int lo = 32 * s_lo, hi = 32 * s_hi - 1;
-  for (int t = s_lo + int(threadIdx.x); t < s_hi; t += NT) {
+  for (int t = s_lo + int(threadIdx.x); t <= s_hi; t += NT) {
+    sm.ch_off[t - s_lo] = a.soff[un.slice0 + t];
+    if (t == s_hi) break;
     const int2 b = a.sbound[un.slice0 + t];
     lo = min(lo, b.x);
     hi = max(hi, b.y);
   }
+  if (threadIdx.x == 0) sm.ch_next = NW;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
@@ -1271,20 +1302,20 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
       if (un.kind == 0) {
         if (PH == PH_INIT) tileI1(x, un, j, ts);
         if (PH == PH_A) {
-          // j: first slice of this warp in the chunk; the chunk's slices
-          // [j - warp, a_end) are dealt round robin (stride NW).
+          // j: the chunk's first slice; its slices [j, a_end) are handed out
+          // to the warps, their sums left in sm.ch_part.
           if (win)
-            tileA1<T, CI, true>(x, un, j, NW, a_end, ts, wbase);
+            tileA1<T, CI, true>(x, un, j, a_end, wbase, sm);
           else
-            tileA1<T, CI, false>(x, un, j, NW, a_end, ts, 0);
+            tileA1<T, CI, false>(x, un, j, a_end, 0, sm);
         }
         if (PH == PH_B) tileB1(x, un, j, ts);
         if (PH == PH_C) {
           if (sm.q_ref[qq]) {
             if (win)
-              tileC1<T, CI, true>(x, un, j, NW, a_end, ts, wbase);
+              tileC1<T, CI, true>(x, un, j, a_end, wbase, sm);
             else
-              tileC1<T, CI, false>(x, un, j, NW, a_end, ts, 0);
+              tileC1<T, CI, false>(x, un, j, a_end, 0, sm);
           } else {
             tileP1(x, un, j);
           }
@@ -1344,11 +1375,20 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
             if (prof) t2 = gtimer();
           }
           if (chunked) {
-            // The chunk's slices, dealt round robin to the warps.
-            const int sl0 = c0 * a.tile_slices + warp;
+            // The chunk's slices, handed out to the warps; then warp 0 adds
+            // their sums in slice order (the same order on every run).
+            const int c_lo = c0 * a.tile_slices;
             a_end = min(un.nslices, c1 * a.tile_slices);
-            if (sl0 < a_end) body(un, qq, sl0, un.row0 + wlo, win);
+            if (c_lo + warp < a_end) body(un, qq, c_lo, un.row0 + wlo, win);
             __syncthreads();
+            if (warp == 0) {
+#pragma unroll
+              for (int s = 0; s < NS; ++s) {
+                double v = 0.0;
+                for (int i = lane; i < a_end - c_lo; i += 32) v += sm.ch_part[s][i];
+                run[s] += warp_total(v);
+              }
+            }
           } else if (warp < c1 - c0) {
             body(un, qq, c0 + warp, 0, false);
           }
