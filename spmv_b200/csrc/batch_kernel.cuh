@@ -312,15 +312,19 @@ __device__ __forceinline__ void prefetch_tile(const V* vals, const CI* idx, int6
 // with slice w), so the warps in flight work on neighbouring slices, whose
 // gathers share lines, and no warp is left with the wide slices of the
 // length-sorted windows while the others wait at the chunk's end.  Up to UA
-// entries per lane are in flight (FP32: 16, one round for most k-NN rows;
-// FP64: 8).
+// entries per lane are in flight (FP32: 14, one round for most k-NN rows;
+// FP64: 8), and each slice's tail (the warp's p.y reduction, the claim of
+// the next slice) overlaps the next slice's loads.
 // WIN: p is read from the CTA's shared-memory window, whose element 0 is
 // p[wbase] (global row index); the window covers every column of the slices.
 template <typename T, typename CI, bool WIN>
 __device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int c_lo, int c_hi,
                                     int64_t wbase, Smem& sm) {
-  constexpr int UA = sizeof(T) == 4 ? 16 : 8;
-  constexpr int UT = sizeof(T) == 4 ? UA / 4 : 0;
+  // Entries per lane in flight: FP32 14 (a remainder of at most 2 takes a
+  // short batch), FP64 8; sizes at which the batch, the next slice's state
+  // and the pending sum stay in registers.
+  constexpr int UA = sizeof(T) == 4 ? 14 : 8;
+  constexpr int UT = sizeof(T) == 4 ? 2 : 0;
   const Args<T, CI>& a = x.a;
   const T* pw = reinterpret_cast<const T*>(bat_dyn + win_offset(a.nunits)) - wbase;
   const int lane = int(threadIdx.x) & 31;
@@ -329,20 +333,30 @@ __device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int c_lo
   const T* __restrict__ pv_ = a.p;
   const int n = c_hi - c_lo;
   int i = int(threadIdx.x) >> 5;
-  while (i < n) {
-    // The next slice is claimed while this one streams.
-    int nxt = 0;
-    if (lane == 0) nxt = atomicAdd(&sm.ch_next, 1);
-    const int64_t e0 = sm.ch_off[i];
-    const int w = int((sm.ch_off[i + 1] - e0) >> 5);
+  if (i >= n) return;
+  // The next slice is claimed, and the previous slice's p.y reduced across
+  // the warp, while this slice's first loads are in flight.
+  int nxt = 0;
+  if (lane == 0) nxt = atomicAdd(&sm.ch_next, 1);
+  int64_t e0 = sm.ch_off[i];
+  int w = int((sm.ch_off[i + 1] - e0) >> 5);
+  double pend = 0.0;
+  int pend_i = -1;
+  auto settle = [&]() {
+    if (pend_i >= 0) {
+      const double t = warp_total(pend);
+      if (lane == 0) sm.ch_part[0][pend_i] = t;
+      pend_i = -1;
+    }
+  };
+  for (;;) {
     const int64_t row = u.row0 + 32 * int64_t(c_lo + i) + lane;
     const T* vp = vals + e0 + lane;
     const CI* ip = idx + e0 + lane;
     T acc = T(0);
     // Every lane loads UA entries (past the slice's width it repeats the last
     // one, so no predicate stays live across the loads and the batch fits the
-    // registers); only the slice's own entries gather p.  FP32: a remainder of
-    // at most UA / 4 entries takes a short batch.
+    // registers); only the slice's own entries gather p.
     for (int k0 = 0; k0 < w; k0 += UA) {
       if (UT > 0 && w - k0 <= UT) {
         T v[UT > 0 ? UT : 1];
@@ -353,6 +367,7 @@ __device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int c_lo
           v[q] = __ldcs(vp + 32 * kk);
           c[q] = ldidx(ip + 32 * kk);
         }
+        settle();
 #pragma unroll
         for (int q = 0; q < UT; ++q)
           if (k0 + q < w) {
@@ -369,6 +384,7 @@ __device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int c_lo
         v[q] = __ldcs(vp + 32 * kk);
         c[q] = ldidx(ip + 32 * kk);
       }
+      settle();
 #pragma unroll
       for (int q = 0; q < UA; ++q)
         if (k0 + q < w) {
@@ -376,12 +392,18 @@ __device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int c_lo
           acc += v[q] * (WIN ? pw[gc] : ld_pol(pv_ + gc, x.keep));
         }
     }
+    settle();
     st_pol(a.y + row, acc, x.keep);
     const T pv = WIN ? pw[row] : ld_pol(pv_ + row, x.keep);
-    const double part = warp_total(double(pv) * double(acc));
-    if (lane == 0) sm.ch_part[0][i] = part;
+    pend = double(pv) * double(acc);
+    pend_i = i;
     i = __shfl_sync(0xffffffffu, nxt, 0);
+    if (i >= n) break;
+    if (lane == 0) nxt = atomicAdd(&sm.ch_next, 1);
+    e0 = sm.ch_off[i];
+    w = int((sm.ch_off[i + 1] - e0) >> 5);
   }
+  settle();
 }
 
 // C, single, refining: r = fl(b - A64 (x + d)); ||r64||^2, r.r, r.p per
