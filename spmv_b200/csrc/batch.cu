@@ -207,10 +207,12 @@ void fill_args(spmv_batch B, Args<T, CI>& a, const SolveIo& io, int kmax, double
   a.rtol2 = rtol * rtol;
   a.delta2 = delta2;
   a.tile_slices = cfg.tile_slices;
-  // The block's tiles against single-unit tiles (4), per phase, from per-CTA
+  // Tile weights against a single unit's tile (8), per phase, from per-CTA
   // phase times on the batched k-NN workload: in FP32 a block tile costs
-  // 0.8x in the product, 1.45x in the alpha update, 1.3x in the p update.
-  a.w = sizeof(T) == 4 ? Weights{6, 12, 10, 128} : Weights{8, 8, 10, 128};
+  // 0.5x a single tile in the product, 1.5x in the alpha update, 1.25x in
+  // the p update; a refinement tile (FP64 product and three sums) 48x a
+  // p-update tile.
+  a.w = sizeof(T) == 4 ? Weights{4, 12, 10, 128, 384} : Weights{8, 8, 10, 128, 384};
   a.nrhs = io.with_block ? B->block_nrhs : 0;
   a.soff = B->soff.as<int64_t>();
   a.sbound = B->sbound.as<int2>();

@@ -47,9 +47,11 @@ struct UnitState {
   int refine_at;  // lockstep iteration of the unit's latest refinement
 };
 
-// Tile weights of the block unit per phase (a single-unit tile weighs 4).
+// Tile weights per phase, in eighths of a single unit's tile (which weighs
+// 8): the block unit's per phase (c2: its refinement) and a single unit's
+// refinement tile.
 struct Weights {
-  int blk_a, blk_b, blk_c, blk_c2;
+  int blk_a, blk_b, blk_c, blk_c2, one_c2;
 };
 
 // Kernel arguments (T: inner precision; CI: int16_t row offsets or int32_t

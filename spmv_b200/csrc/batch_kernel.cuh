@@ -56,12 +56,11 @@ constexpr int U = 8;  // gathers in flight per lane in the products
 // product is latency-bound (two gathered vectors per entry), and block tiles
 // four times as long were slower in every phase.
 constexpr int BT_MUL = 1;
-// Weights in eighths of a single unit's tile in the same phase (a single
-// unit's refinement tile, an FP64 product plus three sums, counts 48 tiles);
-// the block's weights per phase come with the launch (they differ between
-// the precisions), measured per CTA on the batched workload.
+// Weights in eighths of a single unit's tile in the same phase; the
+// refinement tiles' and the block's weights come with the launch (they
+// differ between the precisions), measured per CTA on the batched workload.
 __device__ __forceinline__ int tile_weight(const Weights& w, int ph, int kind, bool refine) {
-  if (ph == PH_C && refine) return kind == 0 ? 8 * 48 : w.blk_c2;
+  if (ph == PH_C && refine) return kind == 0 ? w.one_c2 : w.blk_c2;
   if (kind == 0) return 8;
   return ph == PH_A ? w.blk_a : ph == PH_B ? w.blk_b : ph == PH_C ? w.blk_c : 8;
 }
