@@ -252,7 +252,9 @@ int spmv_matrix_mult_noalloc(spmv_matrix A, const void* const* x,
  * power of two), gathers in flight per lane for SPMV_KERNEL_STAGED (4, 5, 7,
  * 8 or 9; 5, 7 and 9 suit stencils whose rows have a multiple of that many
  * entries: 5-, 7- and 27-point);
- * 0 = from statistics; block: threads per CTA (0 = default). */
+ * 0 = from statistics; block: threads per CTA (0 = default; the staged
+ * product always runs 416-thread CTAs, which get_kernel and the tuner
+ * report). */
 int spmv_matrix_set_kernel(spmv_matrix A, spmv_kernel kernel, int width,
                            int block);
 int spmv_matrix_get_kernel(spmv_matrix A, spmv_kernel* kernel, int* width,

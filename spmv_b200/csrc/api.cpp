@@ -925,7 +925,8 @@ int spmv_matrix_get_kernel(spmv_matrix A, spmv_kernel* kernel, int* width,
       *width = (*kernel == SPMV_KERNEL_SELL || *kernel == SPMV_KERNEL_STAGED)
                    ? 8
                    : auto_width(A->fwd.mean_row, A->dtype);
-    *block = A->block > 0 ? A->block : 256;
+    // Threads per CTA the product runs (the staged product has its own shape).
+    *block = *kernel == SPMV_KERNEL_STAGED ? kStagedThreads : A->block > 0 ? A->block : 256;
   });
 }
 

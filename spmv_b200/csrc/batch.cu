@@ -301,7 +301,7 @@ LaunchCfg resident_cfg(spmv_batch B, spmv_batch_precision prec, LaunchCfg c, con
 
 std::string tune_key(spmv_batch B, int prec) {
   std::ostringstream k;
-  k << "batch:v3:" << prec << ":" << B->nsys << ":" << B->plan.rows_pad << ":" << B->plan.nnz_total << ":"
+  k << "batch:v4:" << prec << ":" << B->nsys << ":" << B->plan.rows_pad << ":" << B->plan.nnz_total << ":"
     << B->plan.entries << ":" << (B->plan.fits16 ? 16 : 32) << ":" << B->block_nrhs << ":"
     << B->block_n;
   return k.str();
@@ -565,21 +565,32 @@ int spmv_batch_autotune(spmv_batch B, spmv_batch_precision prec, spmv_batch_conf
     double pick_us = 0.0;
     int tried = 0;
     if (!cache_lookup(key, pick, pick_us)) {
-      // Right-hand sides of ones, solutions into scratch (every system writes
-      // its own rows of one shared scratch vector, which nothing reads).
+      // One fixed pseudo-random right-hand side in [-1, 1) shared by every
+      // system (splitmix64 of the row index; a vector of ones would not do:
+      // it is an eigenvector of a graph Laplacian plus a diagonal shift, so
+      // CG would stop after one iteration), solutions into scratch (every
+      // system writes its own rows of one shared scratch vector, which
+      // nothing reads).
       const bool blk = B->block_sys >= 0;
       int32_t nmax = 1;
       for (int32_t v : B->plan.n) nmax = std::max(nmax, v);
       const int64_t nbl = blk ? int64_t(B->block_n) * B->block_nrhs : 0;
-      DevBuf ones, scratch, tab;
+      DevBuf rhs, scratch, tab;
       const size_t len = size_t(std::max<int64_t>(nmax, nbl));
-      ones.reserve(sizeof(double) * len);
+      rhs.reserve(sizeof(double) * len);
       scratch.reserve(sizeof(double) * len);
-      std::vector<double> h(len, 1.0);
-      SPMVB_CUDA(cudaMemcpy(ones.ptr, h.data(), sizeof(double) * len, cudaMemcpyHostToDevice));
+      std::vector<double> h(len);
+      for (size_t i = 0; i < len; ++i) {
+        uint64_t z = (uint64_t(i) + 1) * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        h[i] = double(z >> 11) * 0x1.0p-52 - 1.0;
+      }
+      SPMVB_CUDA(cudaMemcpy(rhs.ptr, h.data(), sizeof(double) * len, cudaMemcpyHostToDevice));
       std::vector<const void*> ptrs(2 * std::max(B->nsys, 1));
       for (int i = 0; i < B->nsys; ++i) {
-        ptrs[i] = ones.ptr;
+        ptrs[i] = rhs.ptr;
         ptrs[B->nsys + i] = scratch.ptr;
       }
       tab.reserve(sizeof(void*) * ptrs.size());
@@ -588,7 +599,7 @@ int spmv_batch_autotune(spmv_batch B, spmv_batch_precision prec, spmv_batch_conf
       SolveIo io;
       io.b_user = reinterpret_cast<const double* const*>(tab.ptr);
       io.x_user = reinterpret_cast<double* const*>(tab.as<void*>() + B->nsys);
-      io.B_user = blk ? ones.as<double>() : nullptr;
+      io.B_user = blk ? rhs.as<double>() : nullptr;
       io.X_user = blk ? scratch.as<double>() : nullptr;
       io.with_block = blk;
       cudaEvent_t e0, e1;

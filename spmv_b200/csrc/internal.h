@@ -361,6 +361,9 @@ enum class ProductKind : int {
   Sell = 1,    // SELL-32 from registers, w loads in flight per lane
   Staged = 2,  // SELL-32 staged in shared memory by bulk copies, w gathers per lane
 };
+// Threads per CTA of the staged product (12 consumer warps and a producer
+// warp; a block size given with SPMV_KERNEL_STAGED is not used).
+constexpr int kStagedThreads = 416;
 // Gathers in flight per lane of the staged product: 4, 8, or a stencil's
 // exact row width 5 or 7 (one unmasked chunk per slice).
 inline int staged_width(int w) {

@@ -14,6 +14,9 @@
 #include "spmv_kernel.cuh"
 #include "sell_staged.cuh"
 
+static_assert(spmvb::SolverStaged::BS == spmvb::kStagedThreads,
+              "the staged product's CTA size as reported to callers");
+
 namespace spmvb {
 
 namespace {

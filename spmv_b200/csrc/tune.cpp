@@ -75,7 +75,7 @@ void autotune(spmv_matrix A, int reps, spmv_tune_result* best) {
   if (cache_lookup(key, &r)) {
     A->kernel = r.kernel;
     A->width = r.width;
-    A->block = r.block;
+    A->block = r.kernel == SPMV_KERNEL_STAGED ? 0 : r.block;
     A->kernel_set = false;
     A->cg.reset();
     A->ir.reset();
@@ -176,7 +176,8 @@ void autotune(spmv_matrix A, int reps, spmv_tune_result* best) {
   A->ir.reset();
   r.kernel = best_c.k;
   r.width = best_c.w;
-  r.block = best_c.bs;
+  // Threads per CTA the chosen kernel runs (the staged product's own shape).
+  r.block = best_c.k == SPMV_KERNEL_STAGED ? kStagedThreads : best_c.bs;
   r.us = best_us;
   r.candidates = int(cands.size());
   cache_store(key, r);
