@@ -58,9 +58,10 @@ constexpr int kProfCap = 1 << 16;
 // fallen 100x below its largest value since the last refinement (the
 // reliable-update criterion with delta = 0.01; squared norms compared).
 constexpr double kDelta2 = 1e-4;
-// Rows of p the product phase stages per CTA (64 KB in FP32, 96 KB in FP64:
-// two CTAs per SM still fit).
+// Rows of p the product phase stages per CTA (64 KB in FP32, kept as a ring
+// across a pass's chunks; 88 KB in FP64: two CTAs per SM still fit).
 constexpr int kWinRows32 = 16384;
+static_assert((kWinRows32 & (kWinRows32 - 1)) == 0, "the FP32 window is a ring of 2^k rows");
 constexpr int kWinRows64 = 11264;
 
 // With SPMV_B200_BATCH_PROFILE naming a file, each solve appends one line:

@@ -91,6 +91,9 @@ struct Smem {
   long long ch_off[CH_MAX + 1];
   double ch_part[NSUM][CH_MAX];
   int ch_next;
+  // Global rows [ring_lo, ring_hi] of p held in the FP32 window (empty when
+  // ring_lo > ring_hi); valid within one pass of the product phase.
+  long long ring_lo, ring_hi;
 };
 
 // Dynamic shared memory: the unit list (2 ints per unit), then a region that
@@ -325,7 +328,11 @@ __device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int c_lo
   constexpr int UA = sizeof(T) == 4 ? 14 : 8;
   constexpr int UT = sizeof(T) == 4 ? 2 : 0;
   const Args<T, CI>& a = x.a;
-  const T* pw = reinterpret_cast<const T*>(bat_dyn + win_offset(a.nunits)) - wbase;
+  // FP32: the window is a ring of win_cap (a power of two) rows, row g at
+  // g & (win_cap - 1); FP64: rows from wbase on.
+  constexpr bool RING = sizeof(T) == 4;
+  const T* pw = reinterpret_cast<const T*>(bat_dyn + win_offset(a.nunits)) - (RING ? 0 : wbase);
+  const int64_t wmask = RING ? int64_t(a.win_cap - 1) : int64_t(-1);
   const int lane = int(threadIdx.x) & 31;
   const T* __restrict__ vals = a.vals;
   const CI* __restrict__ idx = a.idx;
@@ -371,7 +378,7 @@ __device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int c_lo
         for (int q = 0; q < UT; ++q)
           if (k0 + q < w) {
             const int64_t gc = gcol<CI>(c[q], row, u.row0);
-            acc += v[q] * (WIN ? pw[gc] : ld_pol(pv_ + gc, x.keep));
+            acc += v[q] * (WIN ? pw[gc & wmask] : ld_pol(pv_ + gc, x.keep));
           }
         break;
       }
@@ -388,12 +395,12 @@ __device__ __noinline__ void tileA1(const Ctx<T, CI>& x, const Unit& u, int c_lo
       for (int q = 0; q < UA; ++q)
         if (k0 + q < w) {
           const int64_t gc = gcol<CI>(c[q], row, u.row0);
-          acc += v[q] * (WIN ? pw[gc] : ld_pol(pv_ + gc, x.keep));
+          acc += v[q] * (WIN ? pw[gc & wmask] : ld_pol(pv_ + gc, x.keep));
         }
     }
     settle();
     st_pol(a.y + row, acc, x.keep);
-    const T pv = WIN ? pw[row] : ld_pol(pv_ + row, x.keep);
+    const T pv = WIN ? pw[row & wmask] : ld_pol(pv_ + row, x.keep);
     pend = double(pv) * double(acc);
     pend_i = i;
     i = __shfl_sync(0xffffffffu, nxt, 0);
@@ -1148,20 +1155,40 @@ __device__ __forceinline__ bool chunk_window(const Args<T, CI>& a, const Unit& u
 }
 
 // Copies p[row0 + wlo, row0 + wlo + wsize) into the window (16-byte steps:
-// row0 is a multiple of 32 and wlo of 4).
+// row0 is a multiple of 32 and wlo of 4).  FP32: the window is a ring (row g
+// at g & (win_cap - 1)) and only the rows it does not hold yet are copied;
+// sm.ring_lo/ring_hi are read here and updated by the caller after the
+// barrier that follows.
 template <typename T, typename CI>
 __device__ __forceinline__ void load_window(const Args<T, CI>& a, const Unit& un, int wlo,
-                                            int wsize) {
+                                            int wsize, const Smem& sm) {
   T* win = reinterpret_cast<T*>(bat_dyn + win_offset(a.nunits));
-  const T* src = a.p + un.row0 + wlo;
-  for (int i0 = 4 * int(threadIdx.x); i0 < wsize; i0 += 4 * 4 * NT) {
-    Four<T> v[4];
+  auto copy = [&](int64_t g0, int64_t g1, int64_t mask, int64_t base) {
+    // Rows [g0, g1) (multiples of 4) to win[(g - base) & mask].
+    const T* src = a.p + g0;
+    const int64_t n = g1 - g0;
+    for (int64_t i0 = 4 * int64_t(threadIdx.x); i0 < n; i0 += 4 * 4 * NT) {
+      Four<T> v[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (i0 + u * 4 * NT < wsize) v[u] = ld4(src + i0 + u * 4 * NT);
+      for (int u = 0; u < 4; ++u)
+        if (i0 + u * 4 * NT < n) v[u] = ld4(src + i0 + u * 4 * NT);
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (i0 + u * 4 * NT < wsize) st4(win + i0 + u * 4 * NT, v[u]);
+      for (int u = 0; u < 4; ++u)
+        if (i0 + u * 4 * NT < n) st4(win + ((g0 + i0 + u * 4 * NT - base) & mask), v[u]);
+    }
+  };
+  const int64_t g0 = un.row0 + wlo, g1 = g0 + wsize;
+  if (sizeof(T) != 4) {
+    copy(g0, g1, int64_t(-1), g0);
+    return;
+  }
+  const int64_t mask = int64_t(a.win_cap - 1);
+  const int64_t r0 = sm.ring_lo, r1 = sm.ring_hi + 1;
+  if (r0 >= r1 || r1 <= g0 || r0 >= g1) {
+    copy(g0, g1, mask, 0);
+  } else {
+    if (g0 < r0) copy(g0, r0, mask, 0);
+    if (r1 < g1) copy(r1, g1, mask, 0);
   }
 }
 
@@ -1236,6 +1263,12 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
     i0 = lo;
   }
   while (i0 < cnt && lw[i0] < Rr) {
+    // The window region also holds the block's sums: the ring of p starts
+    // empty in every pass.
+    if (threadIdx.x == 0) {
+      sm.ring_lo = 1;
+      sm.ring_hi = 0;
+    }
     // Pass table: up to MAXQ consecutive entries this CTA reports for.
     if (warp == 0) {
       int nq = 0, pos = 0, i = i0;
@@ -1373,6 +1406,10 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
         if (un.kind != 0) {
           __syncthreads();
           for (int t = int(threadIdx.x); t < NW * NSUM * BW; t += NT) (&bsum[0][0][0])[t] = 0.0;
+          if (threadIdx.x == 0) {
+            sm.ring_lo = 1;
+            sm.ring_hi = 0;
+          }
           __syncthreads();
         }
         for (int c0 = sm.q_ja[qq]; c0 < sm.q_jb[qq]; c0 += NW) {
@@ -1388,11 +1425,15 @@ __device__ void run_phase(const Ctx<T, CI>& x, int cnt, long long W, const int* 
             if (prof) t1 = gtimer();
             if (win) {
               if (PH == PH_A)
-                load_window(a, un, wlo, wsize);
+                load_window(a, un, wlo, wsize, sm);
               else
                 load_window_xd(a, un, wlo, wsize);
             }
             __syncthreads();
+            if (PH == PH_A && win && threadIdx.x == 0) {
+              sm.ring_lo = un.row0 + wlo;
+              sm.ring_hi = un.row0 + wlo + wsize - 1;
+            }
             if (prof) t2 = gtimer();
           }
           if (chunked) {
