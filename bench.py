@@ -734,9 +734,10 @@ def run_ours(args, info):
                    "traffic_source": "profiles/traffic.json: dram__bytes_read.sum + "
                                      "dram__bytes_write.sum of one launch, committed ncu "
                                      "capture (not measured in this run)",
-                   "kernel": f"cg_fused ({cg_form[1]} CTAs/SM, r in {cg_form[2]}, "
-                             f"staged width {cg_w}, {cg_bits}-bit indices; one launch "
-                             "per solve)",
+                   "kernel": f"cg_fused ({cg_form[1]} CTAs/SM, r in {cg_form[2].split(':')[0]}, "
+                             f"staged width {cg_w}, {cg_bits}-bit indices, "
+                             f"{2 if cg_form[2].endswith(':m') else 3} grid syncs per "
+                             "iteration; one launch per solve)",
                    "bytes_per_launch": matrix_bytes, "us_per_launch": t_launch * 1e6,
                    "bytes_model": "nnz x (8 + index bytes) x iterations",
                    "algorithmic_gbs": cg_ach, "algorithmic_bytes_per_launch": cg_bytes}
@@ -783,7 +784,8 @@ def run_ours(args, info):
                    "product": {"kernel": cg_kind, "width": cg_w, "index_bits": cg_bits,
                                "plain_us": cg_us},
                    "form": {"kind": cg_form[0], "ctas_per_sm": cg_form[1],
-                            "residual_in": cg_form[2]}},
+                            "residual_in": cg_form[2] and cg_form[2].split(":")[0],
+                            "merged_update": bool(cg_form[2] and cg_form[2].endswith(":m"))}},
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             # A graph solve launches an init kernel and three per iteration;

@@ -322,7 +322,9 @@ int spmv_matrix_solver_product(spmv_matrix A, int solver, spmv_kernel* kernel,
 /* How spmv_cg runs on this matrix (chosen by timing when its workspace was
  * built): *fused = 0 for a CUDA graph of three kernels per iteration, 1 for
  * one cooperative launch per solve with *ctas_per_sm persistent CTAs per SM
- * and the residual held in shared memory (*r_shared = 1) or global memory.
+ * and the residual held in shared memory (*r_shared = 1) or global memory,
+ * 2 for the same launch in the merged-update form (two grid syncs per
+ * iteration instead of three).
  * Fails when spmv_cg has not run on the matrix.  No reference counterpart. */
 int spmv_matrix_cg_form(spmv_matrix A, int* fused, int* ctas_per_sm, int* r_shared);
 

@@ -348,14 +348,16 @@ class Matrix:
         """How cg (solver="cg") or cg_mixed (solver="mixed") runs on this
         matrix: ("graph", 0, None) for its kernels in a CUDA graph, or
         ("fused", CTAs per SM, "smem" or "global": where the residual lives)
-        for one cooperative launch per solve; fails if that solver has not
-        run on the matrix."""
+        for one cooperative launch per solve, with ":m" appended for cg's
+        merged-update form (two grid syncs per iteration); fails if that
+        solver has not run on the matrix."""
         fn = {"cg": "spmv_matrix_cg_form", "mixed": "spmv_matrix_cg_mixed_form"}[solver]
         f, cps, rs = C.c_int(), C.c_int(), C.c_int()
         call(fn, self._h, C.byref(f), C.byref(cps), C.byref(rs))
         if not f.value:
             return "graph", 0, None
-        return "fused", cps.value, "smem" if rs.value else "global"
+        where = "smem" if rs.value else "global"
+        return "fused", cps.value, where + (":m" if f.value == 2 else "")
 
     def get_kernel(self):
         k, w, b = C.c_int(), C.c_int(), C.c_int()

@@ -997,7 +997,7 @@ int spmv_matrix_cg_form(spmv_matrix A, int* fused, int* ctas_per_sm, int* r_shar
     check_mat(A);
     require(fused && ctas_per_sm && r_shared, "spmv: NULL output");
     const CgForm f = cg_form(A);
-    *fused = f.fused ? 1 : 0;
+    *fused = f.fused ? (f.merged ? 2 : 1) : 0;
     *ctas_per_sm = f.cps;
     *r_shared = f.rs ? 1 : 0;
   });

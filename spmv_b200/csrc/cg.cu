@@ -63,6 +63,7 @@ struct CgWorkspace {
   const void* fused_fn = nullptr;
   int fused_grid = 0, fused_block = 0, fused_smem = 0, fused_cps = 0;
   bool fused_rs = false;
+  bool fused_mg = false;  // the merged-update form
   spmvb::DevBuf bar, partials2, ctas;
   spmvb::SpmvArgs fused_args;
   const spmvb::StagedDesc* tiles = nullptr;
@@ -271,6 +272,32 @@ __device__ __forceinline__ double cg_fused_product(const SpmvArgs& a, int count,
   return acc;
 }
 
+// Phase A of the merged-update form: y = A p, and this thread's shares of
+// p.y, r.y and y.y (r_at(g): r of the CTA's row g, final for this iteration).
+struct Sums3 {
+  double py, ry, yy;
+};
+template <class CFG, int U, typename CI, class RAt>
+__device__ __forceinline__ Sums3 cg_fused_product3(const SpmvArgs& a, int count, uint64_t q_base,
+                                                   StagedLoop<CFG>& pipe,
+                                                   const unsigned char* smem, int* err,
+                                                   double* __restrict__ y,
+                                                   const double* __restrict__ p, RAt&& r_at) {
+  const uint64_t keep = l2_policy_keep();
+  Sums3 acc{0.0, 0.0, 0.0};
+  staged_loop_consume<CFG, double, CI, U>(
+      a, count, q_base, pipe, smem, err,
+      [&](const PartArg& P, int row, double sum) {
+        const int g = P.row0 + row;
+        st_pol(y + g, sum, keep);
+        acc.py += ld_pol(p + g, keep) * sum;
+        acc.ry += r_at(g) * sum;
+        acc.yy += sum * sum;
+      },
+      XGather<double, true>());
+  return acc;
+}
+
 // Solver scalars of the fused solve (one copy per CTA, in shared memory,
 // written by thread 0 between barriers).
 struct FusedScalars {
@@ -429,7 +456,147 @@ __device__ __forceinline__ bool cg_fused_solve(const CgPtrs& c, const FusedCta& 
   return ok;
 }
 
-template <class CFG, int U, bool D16, bool RS>
+// The merged-update form of the fused solve: two grid syncs per iteration
+// instead of three.  Entering iteration k, r_k, p_k and x_k are final and
+// each CTA holds its share of rr_k = r_k.r_k, summed when r_k was formed.
+//   A  y = A p_k with p.y, r.y and y.y in the product's epilogue; one grid
+//      sum of the four with rr_k.  Every CTA then stops when k > 0 and
+//      rr_k / rr_0 < rtol^2 (x = x_k after k iterations: cg.cpp's test after
+//      its k-th update) or when k = kmax; otherwise alpha = rr_k / p.y and
+//      beta = rr' / rr_k with rr' = rr_k - 2 alpha r.y + alpha^2 y.y, which
+//      is r_{k+1}.r_{k+1} in exact arithmetic.  rr' is formed from this
+//      iteration's true rr_k, so its rounding does not carry over: the
+//      stopping test and the next alpha use the true r.r summed in C.
+//   C  r -= alpha y, x += alpha p, p = p beta + r on the CTA's rows (the same
+//      arithmetic per element as the three-sync form), and the CTA's share
+//      of r.r -> grid barrier (A gathers p).
+// The solve runs one product more than the three-sync form: the one whose
+// sums carry the final r.r.
+template <int NT, int V, class RAt, class Product>
+__device__ __forceinline__ bool cg_fused_solve_merged(const CgPtrs& c, const FusedCta& me,
+                                                      GridSum<NT>& gs, GridSumN<NT, 4>& g4,
+                                                      FusedScalars& sv, RAt&& r_at,
+                                                      Product&& product) {
+  const int tid = int(threadIdx.x);
+  // Init: r = p = b, x = 0, rr_0 = b.b.  Barrier epochs: 1 for the init,
+  // 2k + 2 for iteration k's sum and 2k + 3 for its closing barrier.
+  double rr_part = 0.0;
+  {
+    const uint64_t keep = l2_policy_keep();
+    const int g1 = me.g1;
+    for (int g = me.g0 + tid; g < g1; g += NT) {
+      const double bi = c.b[g];
+      r_at(g) = bi;
+      st_pol(c.p + g, bi, keep);
+      st_pol(c.x + g, 0.0, keep);
+      rr_part += bi * bi;
+    }
+  }
+  double rnorm0 = 0.0;
+  bool ok = coop_grid_sum<NT>(rr_part, c.partials2, c.bar, gridDim.x, &c.st->stage_err,
+                              c.wait_ns, gs, &rnorm0);
+  if (tid == 0) {
+    sv.rtol2 = *static_cast<volatile double*>(&c.st->rtol2);
+    sv.kmax = *static_cast<volatile int*>(&c.st->kmax);
+    sv.rnorm0 = sv.rnorm_old = sv.rnorm_new = rnorm0;
+    sv.alpha = sv.beta = sv.pdoty = 0.0;
+    sv.k = 0;
+    sv.status = SPMV_SUCCESS;
+    sv.go = ok && sv.kmax > 0 && rnorm0 > 0.0 && isfinite(rnorm0);
+  }
+  named_sync(1, NT);
+  int k = 0;
+  while (sv.go) {
+    // A: y = A p, the four sums.
+    const Sums3 s3 = product(k);
+    const double in[4] = {s3.py, s3.ry, s3.yy, rr_part};
+    double tot[4];
+    if (!coop_grid_sum_n<NT, 4>(in, c.partials, c.bar, (2ull * unsigned(k) + 2) * gridDim.x,
+                                &c.st->stage_err, c.wait_ns, g4, tot)) {
+      ok = false;
+      break;
+    }
+    // The stopping test, alpha and beta (one thread; every CTA computes the
+    // same from the same totals).
+    if (tid == 0) {
+      const double rr = tot[3];
+      if (k > 0) {
+        sv.rnorm_new = rr;
+        sv.rnorm_old = rr;
+      }
+      if ((k > 0 && rr / sv.rnorm0 < sv.rtol2) || k >= sv.kmax) {
+        sv.go = false;
+      } else {
+        const double py = tot[0];
+        sv.k = k + 1;
+        sv.pdoty = py;
+        sv.alpha = rr / py;
+        if (py == 0.0 || !isfinite(py)) {
+          sv.status = SPMV_ERROR_BREAKDOWN;
+          sv.go = false;
+        } else {
+          const double a = sv.alpha;
+          const double rr1 = rr - 2.0 * a * tot[1] + a * a * tot[2];
+          sv.beta = rr1 / rr;
+        }
+      }
+    }
+    named_sync(1, NT);
+    if (!sv.go) break;
+
+    // C: r -= alpha y, x += alpha p, p = p beta + r, this CTA's r.r.
+    {
+      const double alpha = sv.alpha, beta = sv.beta;
+      const uint64_t keep = l2_policy_keep();
+      const int g1 = me.g1;
+      rr_part = 0.0;
+      for (int g0 = me.g0 + tid; g0 < g1; g0 += V * NT) {
+        double yv[V], pv[V], xv[V];
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+          const int g = g0 + u * NT;
+          if (g < g1) {
+            yv[u] = ld_pol(c.y + g, keep);
+            pv[u] = ld_pol(c.p + g, keep);
+            xv[u] = ld_pol(c.x + g, keep);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+          const int g = g0 + u * NT;
+          if (g < g1) {
+            const double ri = r_at(g) - alpha * yv[u];
+            r_at(g) = ri;
+            rr_part += ri * ri;
+            st_pol(c.x + g, xv[u] + alpha * pv[u], keep);
+            st_pol(c.p + g, pv[u] * beta + ri, keep);
+          }
+        }
+      }
+    }
+    if (!coop_grid_barrier<NT>(c.bar, (2ull * unsigned(k) + 3) * gridDim.x, &c.st->stage_err,
+                               c.wait_ns, gs)) {
+      ok = false;
+      break;
+    }
+    ++k;
+  }
+  if (tid == 0 && ok && blockIdx.x == 0) {
+    CgState* st = c.st;
+    st->rnorm0 = sv.rnorm0;
+    st->rnorm_old = sv.rnorm_old;
+    st->rnorm_new = sv.rnorm_new;
+    st->alpha = sv.alpha;
+    st->beta = sv.beta;
+    st->pdoty = sv.pdoty;
+    st->k = sv.k;
+    st->status = sv.status;
+  }
+  return ok;
+}
+
+// MG: the merged-update form (two grid syncs per iteration), else three.
+template <class CFG, int U, bool D16, bool RS, bool MG>
 __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
     cg_fused(const __grid_constant__ SpmvArgs a, const CgPtrs c,
              const FusedCta* __restrict__ ctas) {
@@ -463,11 +630,20 @@ __global__ void __launch_bounds__(CFG::BS, CFG::MINB)
   auto r_at = [&](int g) -> double& {
     return RS ? reinterpret_cast<double*>(staged_smem + STAGES_BYTES)[g - me.g0] : c.r[g];
   };
-  cg_fused_solve<NT, V>(c, me, gs, sv, r_at, [&](int k) {
-    const int count = me.t1 - me.t0;
-    return cg_fused_product<CFG, U, CI>(a, count, uint64_t(k) * uint64_t(count), pipe,
-                                        staged_smem, &c.st->stage_err, c.y, c.p);
-  });
+  if constexpr (MG) {
+    __shared__ GridSumN<NT, 4> g4;
+    cg_fused_solve_merged<NT, V>(c, me, gs, g4, sv, r_at, [&](int k) {
+      const int count = me.t1 - me.t0;
+      return cg_fused_product3<CFG, U, CI>(a, count, uint64_t(k) * uint64_t(count), pipe,
+                                           staged_smem, &c.st->stage_err, c.y, c.p, r_at);
+    });
+  } else {
+    cg_fused_solve<NT, V>(c, me, gs, sv, r_at, [&](int k) {
+      const int count = me.t1 - me.t0;
+      return cg_fused_product<CFG, U, CI>(a, count, uint64_t(k) * uint64_t(count), pipe,
+                                          staged_smem, &c.st->stage_err, c.y, c.p);
+    });
+  }
   if (tid == 0) pipe.stop = 1;
 }
 
@@ -482,20 +658,20 @@ using CgFusedTwo = StagedCfg<12, 3, 16384, 2>;
 using CgFusedTwoDeep = StagedCfg<12, 6, 16384, 2>;
 using CgFusedThree = StagedCfg<12, 4, 16384, 3>;
 
-template <class CFG, bool D16, bool RS>
+template <class CFG, bool D16, bool RS, bool MG>
 FusedFn fused_fn_u(int U) {
   switch (staged_width(U)) {
-    case 8: return cg_fused<CFG, 8, D16, RS>;
-    case 9: return cg_fused<CFG, 9, D16, RS>;
-    case 7: return cg_fused<CFG, 7, D16, RS>;
-    case 5: return cg_fused<CFG, 5, D16, RS>;
-    default: return cg_fused<CFG, 4, D16, RS>;
+    case 8: return cg_fused<CFG, 8, D16, RS, MG>;
+    case 9: return cg_fused<CFG, 9, D16, RS, MG>;
+    case 7: return cg_fused<CFG, 7, D16, RS, MG>;
+    case 5: return cg_fused<CFG, 5, D16, RS, MG>;
+    default: return cg_fused<CFG, 4, D16, RS, MG>;
   }
 }
 
-template <class CFG, bool RS>
+template <class CFG, bool RS, bool MG = false>
 FusedFn fused_fn(const SolverProduct& sp) {
-  return sp.d16 ? fused_fn_u<CFG, true, RS>(sp.w) : fused_fn_u<CFG, false, RS>(sp.w);
+  return sp.d16 ? fused_fn_u<CFG, true, RS, MG>(sp.w) : fused_fn_u<CFG, false, RS, MG>(sp.w);
 }
 
 
@@ -673,14 +849,17 @@ void build_graph(spmv_matrix A, CgWorkspace& w) {
 }
 
 // Staged product: shape CFG (CFG::MINB CTAs per SM).
-template <class CFG, bool RS>
+template <class CFG, bool RS, bool MG = false>
 bool plan_fused(spmv_matrix A, const SolverProduct& sp, FusedPlan& plan) {
   static_assert(CFG::max_entries(10) == SolverStaged::max_entries(10) &&
                     CFG::max_entries(12) == SolverStaged::max_entries(12),
                 "fused shapes use the solver product's tiles");
   const int eb = 8 + (sp.d16 ? 2 : 4);
-  return fused_plan(A, cg_tiles(A, sp), (const void*)fused_fn<CFG, RS>(sp), CFG::BS, CFG::MINB,
-                    CFG::smem_bytes(eb), RS ? 8 : 0, plan);
+  if (!fused_plan(A, cg_tiles(A, sp), (const void*)fused_fn<CFG, RS, MG>(sp), CFG::BS,
+                  CFG::MINB, CFG::smem_bytes(eb), RS ? 8 : 0, plan))
+    return false;
+  plan.merged = MG;
+  return true;
 }
 
 void use_plan(CgWorkspace& w, FusedPlan& plan) {
@@ -691,10 +870,11 @@ void use_plan(CgWorkspace& w, FusedPlan& plan) {
   w.fused_smem = plan.smem;
   w.fused_cps = plan.cps;
   w.fused_rs = plan.rs;
-  // One partial per CTA in each reduction's array.  partials is baked into
-  // the graph form's kernels and never reallocated: it was sized for more
-  // CTAs than any plan has.
-  require(w.partials.bytes >= sizeof(double) * size_t(plan.grid),
+  w.fused_mg = plan.merged;
+  // One partial per CTA in each reduction's array (four in partials for the
+  // merged form).  partials is baked into the graph form's kernels and never
+  // reallocated: it was sized for more CTAs than any plan has.
+  require(w.partials.bytes >= sizeof(double) * size_t(plan.grid) * (plan.merged ? 4 : 1),
           "spmv: fused CG grid larger than its partials array");
   w.partials2.reserve(sizeof(double) * size_t(plan.grid));
   w.ctas.reserve(sizeof(FusedCta) * plan.ctas.size());
@@ -765,13 +945,15 @@ float time_iterations(CgWorkspace& w, cudaStream_t s, int its) {
   return best;
 }
 
-// Chooses between the graph form and the fused plans that fit, by timing a
-// few iterations of each on b = 1 (the fused form needs a staged product):
+// Chooses between the graph form and the fused plans that fit, by timing 32
+// iterations of each on b = 1 (the fused form needs a staged product):
 // r in shared memory with one or two CTAs per SM (when the CTAs' rows fit),
-// or r in global memory with two CTAs of 6 stages or three of 4.
-// SPMV_B200_CG_FUSED: "0" keeps the graph form; "<cps>:<smem|global>"
-// forces that plan (1:smem, 2:smem, 1:global, 2:global, 3:global), failing
-// if it does not fit.
+// or r in global memory with two CTAs of 6 stages or three of 4; and the
+// merged-update form (two grid syncs per iteration) of the 2-CTA shared and
+// 3-CTA global plans, whose one extra product per solve weighs 1/32 here.
+// SPMV_B200_CG_FUSED: "0" keeps the graph form; "<cps>:<smem|global>[:m]"
+// forces that plan (1:smem, 2:smem, 1:global, 2:global, 3:global, 2:smem:m,
+// 3:global:m), failing if it does not fit.
 void choose_form(spmv_matrix A, CgWorkspace& w) {
   w.fused = false;
   const SolverProduct& sp = w.product;
@@ -799,22 +981,26 @@ void choose_form(spmv_matrix A, CgWorkspace& w) {
     else if (mode == "1:global") fits = plan_fused<CgFusedOne, false>(A, sp, p);
     else if (mode == "2:global") fits = plan_fused<CgFusedTwoDeep, false>(A, sp, p);
     else if (mode == "3:global") fits = plan_fused<CgFusedThree, false>(A, sp, p);
+    else if (mode == "2:smem:m") fits = plan_fused<CgFusedTwo, true, true>(A, sp, p);
+    else if (mode == "3:global:m") fits = plan_fused<CgFusedThree, false, true>(A, sp, p);
     require(fits, "spmv: SPMV_B200_CG_FUSED must be 0 or a fused plan that fits this matrix "
-                  "(1:smem, 2:smem, 1:global, 2:global, 3:global)");
+                  "(1:smem, 2:smem, 1:global, 2:global, 3:global, 2:smem:m, 3:global:m)");
     use_plan(w, p);
     return;
   }
   std::vector<FusedPlan> plans;
   {
-    FusedPlan p1, p2, p3, p4;
+    FusedPlan p1, p2, p3, p4, p5, p6;
     if (plan_fused<CgFusedOne, true>(A, sp, p1)) plans.push_back(std::move(p1));
     if (plan_fused<CgFusedTwo, true>(A, sp, p2)) plans.push_back(std::move(p2));
     if (plan_fused<CgFusedTwoDeep, false>(A, sp, p3)) plans.push_back(std::move(p3));
     if (plan_fused<CgFusedThree, false>(A, sp, p4)) plans.push_back(std::move(p4));
+    if (plan_fused<CgFusedTwo, true, true>(A, sp, p5)) plans.push_back(std::move(p5));
+    if (plan_fused<CgFusedThree, false, true>(A, sp, p6)) plans.push_back(std::move(p6));
   }
   if (plans.empty()) return;
   cudaStream_t s = A->comm->stream;
-  const int its = 8;
+  const int its = 32;
   SPMVB_CUDA(cudaDeviceSynchronize());
   cg_fill<<<std::max(1, comm->num_sms) * 4, 256, 0, s>>>(w.b.as<double>(), w.n, 1.0);
   SPMVB_CUDA(cudaGetLastError());
@@ -975,6 +1161,7 @@ CgForm cg_form(spmv_matrix A) {
   f.fused = w.fused;
   f.cps = w.fused ? w.fused_cps : 0;
   f.rs = w.fused && w.fused_rs;
+  f.merged = w.fused && w.fused_mg;
   return f;
 }
 

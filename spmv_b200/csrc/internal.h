@@ -408,6 +408,7 @@ struct FusedPlan {
   int grid = 0, block = 0, smem = 0;
   int cps = 0;      // CTAs per SM
   bool rs = false;  // a vector of the CTA's rows kept in shared memory
+  bool merged = false;  // spmv_cg's merged-update form (two grid syncs per iteration)
   std::vector<FusedCta> ctas;
 };
 // A plan for kernel `fn` of `block` threads at `cps` CTAs per SM over the
@@ -424,6 +425,7 @@ struct CgForm {
   bool fused = false;
   int cps = 0;
   bool rs = false;
+  bool merged = false;  // two grid syncs per iteration (spmv_cg's fused form only)
 };
 CgForm cg_form(spmv_matrix A);
 CgForm ir_form(spmv_matrix A);  // spmv_cg_mixed's

@@ -1,7 +1,8 @@
 """The fused CG solve (spmv::cg, cg.cpp:11-83, as one cooperative launch of
 persistent CTAs) against the graph form (three kernels per iteration) on the
-same matrix and staged product, for every fused plan: one or two CTAs per
-SM, the residual in shared or global memory.  Also the reference's edge
+same matrix and staged product, for every fused plan: one, two or three CTAs
+per SM, the residual in shared or global memory, three grid syncs per
+iteration or two (the merged-update form, ":m").  Also the reference's edge
 cases through the fused form: zero right-hand side, the max_its cap,
 breakdown, and run-to-run reproducibility."""
 import numpy as np
@@ -13,7 +14,7 @@ from helpers import build
 
 pytestmark = pytest.mark.gpu
 
-PLANS = ["1:smem", "2:smem", "1:global", "2:global", "3:global"]
+PLANS = ["1:smem", "2:smem", "1:global", "2:global", "3:global", "2:smem:m", "3:global:m"]
 
 
 def setup(monkeypatch, plan, W, P, width=8, kernel="staged"):
@@ -40,13 +41,15 @@ def true_relres(W, x):
                                                ("c2", 32, 8, 7), ("c1", 64, 3, 5),
                                                ("c3", 24, 2, 9)])
 def test_fused_matches_graph_form(monkeypatch, cuda_device, plan, cfg, scale, P, width):
-    """Same per-element arithmetic as the graph form; only the grouping of
-    the two dot products' partial sums differs."""
+    """Same per-element arithmetic as the graph form; the grouping of the
+    dot products' partial sums differs, and the merged-update form takes
+    beta from r.r - 2 alpha r.y + alpha^2 y.y (the next r.r in exact
+    arithmetic)."""
     W = gen.workload(cfg, scale)
     x0, k0, i0, M0 = solve(monkeypatch, "0", W, P, width)
     assert M0.cg_form() == ("graph", 0, None)
     x1, k1, i1, M1 = solve(monkeypatch, plan, W, P, width)
-    cps, where = plan.split(":")
+    cps, where = plan.split(":", 1)
     assert M1.cg_form() == ("fused", int(cps), where)
     assert M1.solver_product("cg")[0] == "staged"
     assert i1.status == 0 and i0.status == 0
@@ -56,7 +59,7 @@ def test_fused_matches_graph_form(monkeypatch, cuda_device, plan, cfg, scale, P,
     assert true_relres(W, x1) < 1.5 * W.rtol
 
 
-@pytest.mark.parametrize("plan", ["1:smem", "2:global"])
+@pytest.mark.parametrize("plan", ["1:smem", "2:global", "2:smem:m"])
 def test_fused_repeats_and_caps(monkeypatch, cuda_device, plan):
     W = gen.workload("c2", 32)
     comm, M, D = setup(monkeypatch, plan, W, 8)
@@ -74,7 +77,7 @@ def test_fused_repeats_and_caps(monkeypatch, cuda_device, plan):
     assert k5 == k1 and all(np.array_equal(a, c) for a, c in zip(x1, x5))
 
 
-@pytest.mark.parametrize("plan", ["1:smem", "2:global"])
+@pytest.mark.parametrize("plan", ["1:smem", "2:global", "2:smem:m"])
 def test_fused_breakdown_is_reported(monkeypatch, cuda_device, plan):
     W = gen.workload("c1", 16)
     zero = gen.CSR(W.A.rowptr, W.A.cols, 0.0 * W.A.vals, W.A.ncols)
@@ -111,7 +114,7 @@ def test_staged_widths_accepted(cuda_device):
         M.set_kernel("sell", 7)
 
 
-@pytest.mark.parametrize("plan", ["2:smem", "3:global"])
+@pytest.mark.parametrize("plan", ["2:smem", "3:global", "2:smem:m"])
 def test_fused_with_an_empty_rank_and_unaligned_ranks(monkeypatch, cuda_device, plan):
     """Ranks of 300, 0 and 724 rows (the last rank's rows start off the
     32-row slice grid; the middle rank owns nothing): the fused solve gives
@@ -136,7 +139,7 @@ def test_fused_with_an_empty_rank_and_unaligned_ranks(monkeypatch, cuda_device, 
 
 
 
-@pytest.mark.parametrize("plan", ["2:smem", "3:global"])
+@pytest.mark.parametrize("plan", ["2:smem", "3:global", "3:global:m"])
 def test_fused_after_set_values(monkeypatch, cuda_device, plan):
     """New values on the same pattern reach the fused solve (its workspace
     keeps its plan and product).  Scaling A by 4 scales every product, alpha

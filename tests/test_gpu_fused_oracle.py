@@ -2,7 +2,8 @@
 restatement of spmv::cg (cg.cpp:11-83) at full size.
 
 FP64 CG: the graph form and every fused plan (one, two or three CTAs per SM;
-the residual in shared or global memory) on the 7-point 128^3 workload over
+the residual in shared or global memory; three grid syncs per iteration, or
+two in the merged-update form, ":m") on the 7-point 128^3 workload over
 8 ranks (rtol 1e-8) and the 5-point 512^2 workload (rtol 1e-8): iterations
 within 2 of the oracle's and x within 1e-9 (relative) of the oracle's x.
 
@@ -22,7 +23,7 @@ from helpers import build
 
 pytestmark = pytest.mark.gpu
 
-CG_PLANS = ["0", "1:smem", "2:smem", "1:global", "2:global", "3:global"]
+CG_PLANS = ["0", "1:smem", "2:smem", "1:global", "2:global", "3:global", "2:smem:m", "3:global:m"]
 MIXED_PLANS = ["0", "2:smem", "2:global", "3:global"]
 
 
