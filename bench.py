@@ -721,7 +721,9 @@ def run_ours(args, info):
         cg_traffic = None
         if tp.exists():
             try:
-                cg_traffic = json.loads(tp.read_text()).get("cg_fused_c2")
+                merged = bool(cg_form[2] and cg_form[2].endswith(":m"))
+                cg_traffic = json.loads(tp.read_text()).get(
+                    "cg_fused_merged_c2" if merged else "cg_fused_c2")
             except Exception:
                 cg_traffic = None
         # achieved / frac count the compulsory DRAM bytes: the matrix stream
