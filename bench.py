@@ -516,33 +516,7 @@ def run_next_rows(device: int, reps: int):
     # create_matrix -----------------------------------------------------------
     nx = 512
     nodes = nx * nx
-    rr = S.owner_ranges(P, nodes)
-    bl, nrl, rgs, cgs = [], [], [], []
-    for r in range(P):
-        r0, r1 = rr[r], rr[r + 1]
-        # Rank r assembles the quads whose lowest node it owns: rows of its own
-        # nodes and of the next grid line (ghost rows owned by rank r + 1).
-        j0, j1 = r0 // nx, min((r1 + nx - 1) // nx, nx - 1)
-        rows = np.arange(j0 * nx, min((j1 + 1) * nx, nodes))
-        ghost_rows = rows[(rows < r0) | (rows >= r1)]
-        rowlist = np.concatenate([np.arange(r0, r1), ghost_rows])
-        # 5-point couplings of each listed row, each entry from two elements
-        # (repeats summed by the assembly).
-        cols, rptr = [], [0]
-        for gr in rowlist:
-            i, j = gr % nx, gr // nx
-            nb = [gr] + [q for q, ok in ((gr - 1, i > 0), (gr + 1, i < nx - 1),
-                                         (gr - nx, j > 0), (gr + nx, j < nx - 1)) if ok]
-            cols.extend(nb + nb)
-            rptr.append(len(cols))
-        cols = np.array(cols, np.int64)
-        gh = np.unique(cols[(cols < r0) | (cols >= r1)])
-        loc = np.where((cols >= r0) & (cols < r1), cols - r0, (r1 - r0) + np.searchsorted(gh, cols))
-        bl.append((np.array(rptr, np.int32), loc.astype(np.int32),
-                   np.full(len(cols), 0.5)))
-        nrl.append(r1 - r0)
-        rgs.append(ghost_rows.astype(np.int64))
-        cgs.append(gh)
+    bl, nrl, rgs, cgs = gen.grid_assembly_5pt(nx, P)
     S.create_matrix(S.Comm(size=P, device=device), bl, nrl, nrl, rgs, cgs)  # warm the path
     t0 = time.perf_counter()
     Ma = S.create_matrix(S.Comm(size=P, device=device), bl, nrl, nrl, rgs, cgs)

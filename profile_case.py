@@ -4,6 +4,7 @@
         [--kernel staged --width 7] [--cg-form 0|2:smem|...]
     python profile_case.py --what batch --count 24 [--precision mixed|fp64]
     python profile_case.py --case c2 --what spmm|bcg|sample|restrict [--nrhs 8]
+    python profile_case.py --what assemble
 
 `matvec` runs the reference matvec demo's loop body (matvecmain.cpp:70-86):
 L2GMap::update then Matrix::mult over all ranks, `reps` times, as plain
@@ -18,7 +19,8 @@ workload with system 0's 32-column block, to 1e-10.  `spmm` runs
 block), `bcg` one block CG solve of `nrhs` columns to the workload's
 tolerance, `sample` `reps` dL/dA samplings (-lambda_i x_j on the pattern),
 `restrict` `reps` passes of transpmult + reverse_update (restrictmain.cpp's
-loop body).
+loop body).  `assemble` runs one create_matrix on the device (Matrix.cpp:
+213-438): the 5-point assembly of a 512^2 node grid over 8 ranks.
 """
 from __future__ import annotations
 
@@ -34,7 +36,7 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--what", default="matvec",
                     choices=["matvec", "cg", "mixed", "batch", "spmm", "bcg", "sample",
-                             "restrict"])
+                             "restrict", "assemble"])
     ap.add_argument("--nrhs", type=int, default=8)
     ap.add_argument("--count", type=int, default=24)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -51,6 +53,17 @@ def main():
     import torch
     import spmv_b200 as S
     from spmv_b200 import gen
+
+    if args.what == "assemble":
+        # One create_matrix on the device: the 5-point assembly of a 512^2
+        # node grid over 8 ranks (repeated couplings summed, ghost rows routed
+        # to their owners).
+        nx, P = 512, 8
+        bl, nrl, rgs, cgs = gen.grid_assembly_5pt(nx, P)
+        M = S.create_matrix(S.Comm(size=P, device=0), bl, nrl, nrl, rgs, cgs)
+        print("assemble", nx, "x", nx, "ranks", P, "entries in",
+              sum(len(b[1]) for b in bl), "out", sum(M.nnz(q) for q in range(P)))
+        return
 
     if args.what == "batch":
         from spmv_b200.core import Batch

@@ -258,3 +258,37 @@ def c4_block_rhs(n: int, nrhs: int = 32, seed: int = 3):
     n x nrhs, row-major, column l ~ N(0,1) from stream 400 + l."""
     return np.ascontiguousarray(np.stack([normal(seed, 400 + l, n) for l in range(nrhs)],
                                          axis=1))
+
+
+def grid_assembly_5pt(nx: int, P: int):
+    """Input of create_matrix (Matrix.cpp:213-438) for a 5-point assembly on
+    an nx x nx node grid over P ranks: rank r lists the rows of its own nodes
+    and of the next grid line (ghost rows owned by rank r + 1), each coupling
+    entered twice (from two elements; the assembly sums repeats), value 0.5.
+    Returns (blocks, nrows_local, row_ghosts, col_ghosts) as create_matrix
+    takes them."""
+    nodes = nx * nx
+    rr = owner_ranges(P, nodes)
+    bl, nrl, rgs, cgs = [], [], [], []
+    for r in range(P):
+        r0, r1 = rr[r], rr[r + 1]
+        j0, j1 = r0 // nx, min((r1 + nx - 1) // nx, nx - 1)
+        rows = np.arange(j0 * nx, min((j1 + 1) * nx, nodes))
+        ghost_rows = rows[(rows < r0) | (rows >= r1)]
+        rowlist = np.concatenate([np.arange(r0, r1), ghost_rows])
+        cols, rptr = [], [0]
+        for gr in rowlist:
+            i, j = gr % nx, gr // nx
+            nb = [gr] + [q for q, ok in ((gr - 1, i > 0), (gr + 1, i < nx - 1),
+                                         (gr - nx, j > 0), (gr + nx, j < nx - 1)) if ok]
+            cols.extend(nb + nb)
+            rptr.append(len(cols))
+        cols = np.array(cols, np.int64)
+        gh = np.unique(cols[(cols < r0) | (cols >= r1)])
+        loc = np.where((cols >= r0) & (cols < r1), cols - r0,
+                       (r1 - r0) + np.searchsorted(gh, cols))
+        bl.append((np.array(rptr, np.int32), loc.astype(np.int32), np.full(len(cols), 0.5)))
+        nrl.append(int(r1 - r0))
+        rgs.append(ghost_rows.astype(np.int64))
+        cgs.append(gh)
+    return bl, nrl, rgs, cgs
